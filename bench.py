@@ -1,0 +1,389 @@
+"""Benchmark: G pair-interactions/s of the Hermite-4 step on one B200.
+
+Workload (default): Plummer sphere N = 65536 (Henon units, seed 1), softening
+eps = 1e-2, shared fixed dt = 1/1024; one step = predict + acc/jerk of all N^2
+pairs + correct, replayed from the engine's captured CUDA graph.  The headline
+`value` is the mixed-precision path (FP32 pair loop on hi/lo positions, FP64
+accumulation and integration); the plain FP64 path runs on the same input
+and is reported beside it with both runs' |dE/E|.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own FP64 CPU code (compiled from its
+sources into oracle/_ref) on this host's cores: each step is one fixed-dt
+Hermite step whose force evaluation computes the share of i-rows that rank 0
+of an S-rank job owns (the reference's own decomposition, src/kernel.cpp:1185),
+with S sized to bound the run; the full-step time is S x that force time plus
+the unsampled O(N) phases.
+
+Multi-GPU (torchrun): replicas only - every rank runs the same independent
+system on its own GPU with no data exchange; value = ranks x N^2 / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "n-body-code_b200"))
+
+METRIC = "Gpair-interactions/s at N=65536: mixed-prec vs FP64 GPU, equal energy error"
+FLOP_PER_INTERACTION = 60
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--n", type=int, default=65536)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--eps", type=float, default=1e-2)
+    ap.add_argument("--dt", type=float, default=1.0 / 1024)
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"))
+    ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison arm")
+    ap.add_argument("--tune", action="store_true", help="autotune pair-kernel tiling first")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload_name(a, precision):
+    return (f"Hermite-4 shared fixed step, Plummer N={a.n} seed {a.seed} (Henon units), "
+            f"eps={a.eps:g}, dt=1/{round(1 / a.dt)}, {precision}")
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for _, _, r in rows for k, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def traffic_per_launch(precision):
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pair_kernel_dram.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(precision)
+    except (OSError, ValueError):
+        return None
+
+
+def run_arm(a, precision, state, torch, dist, rank, world, dev):
+    import nbody_b200 as nb
+    n = a.n
+    e = nb.Engine(n, eps2=a.eps ** 2, precision=precision, device=dev, dt=a.dt, tune=a.tune)
+    e.set_state(state)
+    e.force_calculation()
+    T0, U0 = e.energy()
+    stream = torch.cuda.ExternalStream(e.stream, device=f"cuda:{dev}")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{dev}")
+    e.timestepping(a.warmup)
+    e.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    pair_ms, pred_ms, corr_ms = [], [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream), ClockSampler(dev) as clk:
+        for k in range(a.steps):
+            flush.zero_()                       # evict L2 between timed steps
+            starts[k].record(stream)
+            e.timestepping(1)
+            ends[k].record(stream)
+            ends[k].synchronize()
+            t = e.timers()                      # graph-internal events of this step
+            pred_ms.append(t["pred_ms"]); pair_ms.append(t["eval_ms"]); corr_ms.append(t["corr_ms"])
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(t) for s, t in zip(starts, ends)]
+    tm = e.timers()
+    T1, U1 = e.energy()
+    de = abs((T1 + U1) - (T0 + U0)) / abs(T0 + U0)
+    e.close()
+    return {
+        "ms_per_step": float(np.mean(step_ms)),
+        "pair_ms": float(np.mean(pair_ms)),
+        "pred_ms": float(np.mean(pred_ms)),
+        "corr_ms": float(np.mean(corr_ms)),
+        "dE_over_E": de,
+        "E0": T0 + U0,
+        "tiling": {k: tm[k] for k in ("threads", "i_per_thread", "j_tile", "split_j")},
+        "clocks": clk.summary(),
+        "launches": 3 * a.steps,
+    }
+
+
+def run_e2e(a, precision, state, torch, steps):
+    """End to end through the drop-in C-ABI call (the reference's
+    force_calculation contract): pinned host arrays in, host arrays out,
+    host<->device copies inside every timed call."""
+    import nbody_b200 as nb
+    n = a.n
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(state[k])).pin_memory() for k in nb.FIELDS}
+    host = {k: v.numpy() for k, v in pinned.items()}
+    out_t = torch.empty((6, n), dtype=torch.float64).pin_memory()
+    import ctypes as C
+    from nbody_b200 import _lib
+    L = _lib.load()
+    ptrs = [C.c_void_p(host[k].ctypes.data) for k in nb.FIELDS]
+    outs = [C.c_void_p(out_t[k].data_ptr()) for k in range(6)]
+    prec = 1 if precision == "mixed" else 0
+
+    def call():
+        _lib.check(L.nbody_force_calculation(n, a.eps ** 2, prec, 0, n, *ptrs, *outs),
+                   "nbody_force_calculation")
+
+    for _ in range(2):
+        call()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        call()
+        ts.append(time.perf_counter() - t0)
+    nb.release_force_cache()
+    s = float(np.mean(ts))
+    return {"value": n * n / s / 1e9, "unit": "Gint/s", "h2d_bytes_per_step": 7 * 8 * n,
+            "d2h_bytes_per_step": 6 * 8 * n, "ms_per_call": s * 1e3,
+            "what": "nbody_force_calculation (drop-in for force_calculation), pinned host buffers"}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own code (oracle/_ref) or, if absent, the oracle port
+# ---------------------------------------------------------------------------
+def cpu_reference_steps(a, state, nsteps, seconds_per_step):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n = a.n
+    if not O.have_reference():
+        return None
+    lib = O.ref()
+    cores = lib.ref_max_threads()
+    arrs = [np.ascontiguousarray(state[k]) for k in ("x", "y", "z", "m", "vx", "vy", "vz")]
+    P = O._p
+    # calibrate the sample: one step with a small share, then size S
+    s_cal = 4096
+    h = lib.ref_bench_create(n, a.dt, s_cal, *map(P, arrs))
+    t3 = np.zeros(3)
+    lib.ref_bench_step(h, P(t3))
+    lib.ref_bench_destroy(h)
+    full_force = max(t3[1] * s_cal, 1e-6)
+    S = int(min(4096, max(1, round(full_force / seconds_per_step))))
+    h = lib.ref_bench_create(n, a.dt, S, *map(P, arrs))
+    steps = []
+    for _ in range(nsteps):
+        lib.ref_bench_step(h, P(t3))
+        steps.append(t3.copy())
+    lib.ref_bench_destroy(h)
+    st = np.array(steps)
+    step_s = st[:, 0] + S * st[:, 1] + st[:, 2]
+    return {"per_step_s": step_s, "force_sample_s": st[:, 1], "S": S, "cores": cores,
+            "kind": "reference",
+            "sample": (f"reference FP64 CPU build (oracle/_ref), N={n}: each step = prediction + "
+                       f"force_calculation on rank 0's 1/{S} share of i-rows (src/kernel.cpp:1185) "
+                       f"+ snapandcrackle + correction; full step = pred + {S} x force + corr")}
+
+
+def cpu_port_steps(a, state, nsteps, seconds_per_step):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n = a.n
+    rows_per_s = 2e8 / n  # rough single-thread rate of the direct row sum
+    nrows = int(max(8, min(n, rows_per_s * seconds_per_step)))
+    rows = np.linspace(0, n - 1, nrows).astype(np.int32)
+    ts = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        O.force_rows(state, a.eps ** 2, rows)
+        ts.append(time.perf_counter() - t0)
+    per = np.array(ts) * (n / nrows)
+    return {"per_step_s": per, "S": n / nrows, "cores": 1, "kind": "port",
+            "sample": f"oracle direct row sums on {nrows} of {n} rows per step, scaled by N/rows"}
+
+
+def cpu_baseline(a, state):
+    r = cpu_reference_steps(a, state, 3, a.cpu_sample_seconds / 3) or \
+        cpu_port_steps(a, state, 3, a.cpu_sample_seconds / 3)
+    v = a.n * a.n / float(np.mean(r["per_step_s"])) / 1e9
+    return {"value": v, "unit": "Gint/s", "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def main_reference(a):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    import nbody_b200 as nb  # host-only: the Plummer generator
+    state = nb.plummer(a.n, a.seed)
+    total = a.steps + a.warmup
+    per_step_budget = min(2.0, max(0.2, 150.0 / max(total, 1)))
+    r = cpu_reference_steps(a, state, total, per_step_budget)
+    if r is None:
+        r = cpu_port_steps(a, state, total, per_step_budget)
+    timed = r["per_step_s"][a.warmup:]
+    s = float(np.mean(timed))
+    v = a.n * a.n / s / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gint/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer sphere)",
+        "config": {"workload": workload_name(a, "FP64 CPU (reference)"), "n": a.n,
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": v, "unit": "Gint/s", "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"]},
+        "e2e": {"value": v, "unit": "Gint/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return main_reference(a)
+    import torch
+    world, rank, local = dist_setup()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    dev = local
+    torch.cuda.set_device(dev)
+    import nbody_b200 as nb
+    state = nb.plummer(a.n, a.seed)
+    peaks = nb.measure_peaks(dev)
+    main_arm = run_arm(a, a.precision, state, torch, dist, rank, world, dev)
+    other = None
+    other_prec = "fp64" if a.precision == "mixed" else "mixed"
+    if not a.no_fp64_arm:
+        other = run_arm(a, other_prec, state, torch, dist, rank, world, dev)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = max_over_ranks(main_arm["ms_per_step"])
+    pair_ms = max_over_ranks(main_arm["pair_ms"])
+    e2e = run_e2e(a, a.precision, state, torch, max(3, min(a.steps, 20)))
+    e2e["value"] = e2e["value"] * world
+    cpu = cpu_baseline(a, state) if (rank == 0 and world == 1) else None
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        dist.destroy_process_group()
+        return 0
+    inter = float(a.n) * a.n
+    value = world * inter / (ms * 1e-3) / 1e9
+
+    def roofline(arm, prec):
+        peak = peaks["fp32_tflops"] if prec == "mixed" else peaks["fp64_tflops"]
+        achieved = FLOP_PER_INTERACTION * inter / (arm["pair_ms"] * 1e-3) / 1e12
+        return {"bound": "fp32" if prec == "mixed" else "fp64", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic_per_launch(prec),
+                "kernel": f"pair_{'mixed' if prec == 'mixed' else 'fp64'}_kernel",
+                "peak_source": "measured live by nbody_measure_peaks (FMA microkernel, this GPU)",
+                "flop_per_interaction": FLOP_PER_INTERACTION}
+
+    main_arm["pair_ms"] = pair_ms
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gint/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
+        "data": "synthetic (seeded Plummer sphere, Henon units)",
+        "config": {"workload": workload_name(a, a.precision), "n": a.n, "eps": a.eps, "dt": a.dt,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MiB write, untimed)"},
+        "roofline": roofline(main_arm, a.precision),
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": main_arm["launches"],
+        "clocks": main_arm["clocks"],
+        "phases_ms": {"pred": main_arm["pred_ms"], "eval": main_arm["pair_ms"], "corr": main_arm["corr_ms"]},
+        "tiling": main_arm["tiling"],
+        "energy_error": {a.precision: main_arm["dE_over_E"]},
+        "peaks_measured": peaks,
+    }
+    if other is not None:
+        ov = world * inter / (max_over_ranks(other["ms_per_step"]) * 1e-3) / 1e9
+        line[other_prec] = {"value": ov, "ms_per_step": other["ms_per_step"], "pair_ms": other["pair_ms"],
+                            "roofline": roofline(other, other_prec), "tiling": other["tiling"],
+                            "clocks": other["clocks"]}
+        line["energy_error"][other_prec] = other["dE_over_E"]
+        line["mixed_over_fp64"] = (value / ov) if a.precision == "mixed" else (ov / value)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+/*
+ * nbody_cuda.h - C-ABI of the B200 (sm_100a) direct-summation Hermite-4
+ * N-body engine (libnbody_cuda.so).
+ *
+ * This header replaces the reference's force back-end interface:
+ *   include/kernel.h:15-19        void force_calculation(13 x double*, Sys&)
+ *   include/nbody_tt_integration.h  (TT-Metal host API plumbing)
+ *   src/kernel.cpp:47-1224        five #if-selected force_calculation bodies
+ * and exposes, as device kernels, the O(N) Hermite pieces of
+ *   src/nbody.cpp:131-222         initialdt, prediction, snapandcrackle,
+ *                                 correction, updatedt
+ *   src/utils.cpp:125-153         compute_kinetic, compute_potential
+ *
+ * Conventions
+ *   - Every entry returns nbody_status; no exception crosses the boundary.
+ *     nbody_last_error() returns a thread-local message for the last failure.
+ *   - Host arrays are borrowed for the duration of a call only.  The engine
+ *     owns its device memory from nbody_create to nbody_destroy; no entry
+ *     point allocates after nbody_create (the autotuner, graph capture and
+ *     ensemble set-up allocate once, on first use).
+ *   - An engine is not thread-safe; it serialises all work on its own CUDA
+ *     stream.  Several engines may coexist.
+ *   - Array layout is SoA float64: x, y, z, m, vx, vy, vz and ax, ay, az,
+ *     jx, jy, jz ("jerk" = adot in the reference's names).
+ *   - Physics: G = 1.  a_i = sum_j m_j r_ij / (r_ij^2 + eps2)^(3/2),
+ *     r_ij = x_j - x_i; jerk_i = sum_j m_j [v_ij / (.)^(3/2)
+ *     - 3 (r_ij . v_ij) r_ij / (.)^(5/2)]  (src/kernel.cpp:1187-1221).
+ *     The self term (j = i) contributes exactly zero when eps2 > 0.
+ */
+#ifndef NBODY_CUDA_H
+#define NBODY_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  NBODY_OK = 0,
+  NBODY_ERR_INVALID_ARG = 1, /* bad size, null pointer, eps2 out of range ... */
+  NBODY_ERR_OOM = 2,         /* device or pinned allocation failed at create */
+  NBODY_ERR_CUDA = 3,        /* a CUDA runtime call failed                   */
+  NBODY_ERR_TIMEOUT = 4,     /* a bounded in-kernel wait gave up             */
+  NBODY_ERR_NONFINITE = 5,   /* NaN/Inf in a diagnostic                      */
+  NBODY_ERR_NO_DEVICE = 6,   /* no sm_100 device visible                     */
+  NBODY_ERR_STATE = 7        /* call order (e.g. step before set_state)      */
+} nbody_status;
+
+typedef enum {
+  NBODY_FP64 = 0,  /* all-FP64 pair loop                                     */
+  NBODY_MIXED = 1  /* FP32 pair loop on hi/lo positions, FP64 accumulation   */
+} nbody_precision;
+
+typedef struct {
+  int n;              /* bodies, >= 1                                       */
+  double eps2;        /* softening^2, 1e-30 <= eps2 <= 1e30 (runtime; the
+                         reference hard-codes 1e-7: include/kernel.h:13)    */
+  int precision;      /* nbody_precision                                    */
+  int device;         /* CUDA ordinal                                       */
+  double dt;          /* > 0: fixed shared step; <= 0: adaptive (Aarseth,
+                         src/nbody.cpp:131-150, 198-222)                    */
+  double eta;         /* adaptive criterion, default 1e-2 (nbody.h:16)      */
+  double eta0;        /* initial-dt criterion, default 1e-4 (nbody.h:15)    */
+  int tune;           /* 1: time candidate tilings on first use (autotuner) */
+  int threads, i_per_thread, j_tile, split_j; /* 0 = choose automatically   */
+} nbody_config;
+
+typedef struct nbody_engine nbody_engine;
+
+typedef struct {
+  double pred_ms, eval_ms, corr_ms; /* last step, CUDA events: the reference's
+                                       PRED / EVAL / CORR columns
+                                       (src/main.cpp:107-116)               */
+  double eval_init_ms;              /* first force evaluation               */
+  int num_sms;
+  int threads, i_per_thread, j_tile, split_j; /* tiling in use          */
+  long long steps;                  /* Hermite steps taken                  */
+  double t, dt;                     /* model time and current shared dt     */
+} nbody_timers;
+
+/* Fill *cfg with defaults: eps2 = 1e-7, FP64, device 0, adaptive dt,
+ * eta = 1e-2, eta0 = 1e-4, no tuning, automatic tiling. */
+nbody_status nbody_config_init(nbody_config* cfg);
+
+nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg);
+nbody_status nbody_destroy(nbody_engine* eng);
+
+/* Upload x..vz (n each).  Resets model time and the derivative state. */
+nbody_status nbody_set_state(nbody_engine* eng, const double* x, const double* y,
+                             const double* z, const double* m, const double* vx,
+                             const double* vy, const double* vz);
+/* Download positions and velocities (any pointer may be NULL to skip). */
+nbody_status nbody_get_state(nbody_engine* eng, double* x, double* y, double* z, double* vx,
+                             double* vy, double* vz);
+/* Download the current acc and jerk (any pointer may be NULL). */
+nbody_status nbody_get_derivs(nbody_engine* eng, double* ax, double* ay, double* az,
+                              double* jx, double* jy, double* jz);
+
+/* Evaluate acc + jerk of the current state into the engine's derivative
+ * arrays (the force_calculation equivalent; include/kernel.h:15-19).  In
+ * adaptive mode also sets dt from the initial criterion (initialdt). */
+nbody_status nbody_acc_jerk(nbody_engine* eng);
+
+/* The three Hermite phases, individually (src/nbody.cpp:152-196):
+ * predict x, v in place; evaluate acc/jerk of the predicted state into the
+ * engine's new-derivative buffer; correct with snap/crackle and adopt the
+ * new derivatives (and the Aarseth dt in adaptive mode). */
+nbody_status nbody_predict(nbody_engine* eng);
+nbody_status nbody_eval_predicted(nbody_engine* eng);
+nbody_status nbody_correct(nbody_engine* eng);
+
+/* nsteps complete Hermite steps (predict, evaluate, correct), replayed from
+ * a captured CUDA graph.  Calls nbody_acc_jerk first if no derivatives
+ * exist yet.  Asynchronous: returns once enqueued. */
+nbody_status nbody_step(nbody_engine* eng, int nsteps);
+nbody_status nbody_synchronize(nbody_engine* eng);
+
+/* FP64 kinetic and potential energy of the current state, G = 1,
+ * U = -sum_{i<j} m_i m_j / sqrt(r^2 + eps2).  ref_compat = 1 reproduces the
+ * reference's printed potential, which uses m_j*m_j (src/utils.cpp:148). */
+nbody_status nbody_energy(nbody_engine* eng, int ref_compat, double* T, double* U);
+
+nbody_status nbody_get_timers(nbody_engine* eng, nbody_timers* out);
+/* The engine's CUDA stream (cudaStream_t), for callers that order their own
+ * work against it. */
+nbody_status nbody_get_stream(nbody_engine* eng, void** stream);
+
+const char* nbody_last_error(void);
+const char* nbody_status_string(nbody_status s);
+
+/* ---- the drop-in for the reference's force back end ------------------------
+ * Same arguments and meaning as force_calculation (include/kernel.h:15-19):
+ * reads x, y, z, m, vx, vy, vz (host), zeroes the six outputs and writes the
+ * acc and jerk of i-rows [i_begin, i_end) against all n bodies; rows outside
+ * the range stay zero, so an MPI caller that sums ranks (src/nbody.cpp:
+ * 240-246) gets the complete result.  A cached engine per (thread, device)
+ * is reused, so repeated calls allocate nothing after the first.  Copies
+ * host->device and back inside the call (the reference contract). */
+nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin, int i_end,
+                                     const double* x, const double* y, const double* z,
+                                     const double* m, const double* vx, const double* vy,
+                                     const double* vz, double* ax, double* ay, double* az,
+                                     double* jx, double* jy, double* jz);
+/* Release the cached drop-in engines of the calling thread. */
+nbody_status nbody_force_calculation_release(void);
+
+/* ---- device-pointer entry (zero-copy; used by the torch binding) ----------
+ * Same physics on caller-owned device arrays (float64, n each, on the
+ * engine's device); work is ordered on `stream` (cudaStream_t, NULL = the
+ * engine's stream).  eng supplies eps2, precision, tiling and scratch; n must
+ * be <= the engine's n. */
+nbody_status nbody_acc_jerk_device(nbody_engine* eng, int n, const double* x, const double* y,
+                                   const double* z, const double* m, const double* vx,
+                                   const double* vy, const double* vz, double* ax, double* ay,
+                                   double* az, double* jx, double* jy, double* jz,
+                                   void* stream);
+
+/* ---- initial conditions (host, deterministic) ------------------------------
+ * Plummer sphere in Henon units (G = M = 1, E = -1/4), equal masses 1/n,
+ * centred on the origin in position and velocity; sampled by the
+ * Aarseth-Henon-Wielen (1974) method from a seeded xoshiro256** stream. */
+nbody_status nbody_plummer(int n, uint64_t seed, double* x, double* y, double* z, double* m,
+                           double* vx, double* vy, double* vz);
+/* The reference's own initial conditions (src/nbody.cpp:69-114: std::mt19937
+ * seed 42, vmax = rmax = mmax = 1, mmin = 0.01, virial rescale with the
+ * reference potential at eps2) - the config-1 bodies. */
+nbody_status nbody_reference_ic(int n, double eps2, double* x, double* y, double* z, double* m,
+                                double* vx, double* vy, double* vz);
+
+/* ---- measured pipe peaks (diagnostic) ---------------------------------------
+ * Times FP64 FMA, FP32 FMA and MUFU rsqrt throughput on `device` with
+ * dependent-chain-free microkernels; results in op/s (an FMA counts 2 flop
+ * in the *_tflops fields). */
+typedef struct {
+  double fp64_tflops, fp32_tflops, fp32x2_tflops, mufu_rsqrt_gops;
+  double sm_clock_mhz; /* cudaDevAttrClockRate at the time of the call */
+} nbody_peaks;
+nbody_status nbody_measure_peaks(int device, nbody_peaks* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBODY_CUDA_H */

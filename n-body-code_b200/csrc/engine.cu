@@ -1,0 +1,772 @@
+// libnbody_cuda: the engine behind include/nbody_cuda.h.
+//
+// One engine = one system of n bodies on one device, one CUDA stream, and
+// device memory allocated once at creation:
+//   state  [13][ld] float64  X(3) V(3) M(1) D(6)  (D = current acc, jerk)
+//   P      [S][6][ld]        split-j partial sums of the pair kernel
+//   jb64   [ld] JBody64      FP64 j-records (also used by the potential)
+//   jb32   [ld] JBody32      mixed-precision j-records (mixed engines)
+//   ctl    StepCtl           dt, t, Aarseth criterion, step counter
+// ld = n rounded up to a multiple of 256 (kPad).
+//
+// A Hermite step is three launches - predict (O(N), writes the j-records),
+// pair (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
+// correction + dt criterion) - captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/nbody_cuda.h"
+#include "hermite.cuh"
+#include "pair.cuh"
+
+using namespace nbody;
+
+namespace {
+
+constexpr int kPad = 256;        // body padding granularity (multiple of every j-tile)
+constexpr int kMaxSplit = 64;    // split-j upper bound
+constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
+
+thread_local std::string g_last_error;
+
+nbody_status fail(nbody_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define NB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? NBODY_ERR_OOM : NBODY_ERR_CUDA,          \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+#define NB_TRY(expr)                 \
+  do {                               \
+    nbody_status s_ = (expr);        \
+    if (s_ != NBODY_OK) return s_;   \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Pair-kernel registry: every compiled (precision, NT, IPT, TJ) instantiation.
+// ---------------------------------------------------------------------------
+struct PairKernel {
+  int precision, nt, ipt, tj;
+  const void* fn;
+  size_t smem;  // dynamic shared memory: two j-tile buffers
+  size_t rec;   // bytes per j-record
+};
+
+template <int NT, int IPT, int TJ>
+PairKernel make_fp64() {
+  return {NBODY_FP64, NT, IPT, TJ, reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ>),
+          2 * TJ * sizeof(JBody64), sizeof(JBody64)};
+}
+template <int NT, int IPT, int TJ>
+PairKernel make_mixed() {
+  return {NBODY_MIXED, NT, IPT, TJ, reinterpret_cast<const void*>(&pair_mixed_kernel<NT, IPT, TJ>),
+          2 * TJ * sizeof(JBody32), sizeof(JBody32)};
+}
+
+const std::vector<PairKernel>& registry() {
+  static const std::vector<PairKernel> r = {
+      make_fp64<128, 1, 128>(),  make_fp64<128, 2, 128>(),  make_fp64<128, 4, 128>(),
+      make_fp64<256, 1, 128>(),  make_fp64<256, 2, 128>(),  make_fp64<128, 2, 256>(),
+      make_fp64<64, 2, 128>(),   make_fp64<64, 4, 128>(),
+      make_mixed<128, 1, 128>(), make_mixed<128, 2, 128>(), make_mixed<128, 4, 128>(),
+      make_mixed<256, 2, 128>(), make_mixed<128, 4, 256>(), make_mixed<256, 4, 256>(),
+      make_mixed<64, 4, 128>(),  make_mixed<128, 2, 256>(),
+  };
+  return r;
+}
+
+const PairKernel* find_kernel(int precision, int nt, int ipt, int tj) {
+  for (const auto& k : registry())
+    if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj) return &k;
+  return nullptr;
+}
+
+struct Tiling {
+  const PairKernel* k = nullptr;
+  int split = 1;
+};
+
+// Autotune results shared by all engines of the process: (device, precision,
+// ld, rows) -> tiling.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;  // -> (kernel idx, split)
+
+}  // namespace
+
+struct nbody_engine {
+  nbody_config cfg{};
+  int n = 0, ld = 0, dev = 0, num_sms = 0;
+  cudaStream_t stream = nullptr;
+  double* state = nullptr;  // [13][ld]
+  double *X = nullptr, *V = nullptr, *M = nullptr, *D = nullptr;
+  double* P = nullptr;
+  int p_splits = 0;
+  JBody64* jb64 = nullptr;
+  JBody32* jb32 = nullptr;
+  StepCtl* ctl = nullptr;
+  double* partial = nullptr;  // reduction scratch: ld / 256 + 1 doubles + 4 scalars
+  int* status = nullptr;
+  Tiling tiling;
+  bool tiled = false;
+  cudaGraphExec_t graph = nullptr;
+  bool have_state = false, have_derivs = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_init[2] = {nullptr, nullptr};
+  bool step_events = false, init_events = false;
+};
+
+namespace {
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+nbody_status check_status_word(nbody_engine* e) {
+  int h = 0;
+  NB_CUDA(cudaMemcpyAsync(&h, e->status, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  if (h == kKernelTimeout) {
+    cudaMemsetAsync(e->status, 0, sizeof(int), e->stream);
+    return fail(NBODY_ERR_TIMEOUT, "a pair-kernel shared-memory wait exceeded its limit");
+  }
+  return NBODY_OK;
+}
+
+// Split count from a wave model: CTAs = i_blocks * S run in waves of
+// (SMs x resident CTAs); each CTA costs its j-tiles plus a fixed overhead.
+int choose_split(const nbody_engine* e, const PairKernel& k, int rows) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, k.nt, k.smem) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  const long slots = static_cast<long>(e->num_sms) * occ;
+  const long i_blocks = (rows + k.nt * k.ipt - 1) / (k.nt * k.ipt);
+  const int n_tiles = e->ld / k.tj;
+  double best = 1e300;
+  int best_s = 1;
+  for (int s = 1; s <= std::min(kMaxSplit, n_tiles); ++s) {
+    const long ctas = i_blocks * s;
+    const long waves = (ctas + slots - 1) / slots;
+    const int tps = (n_tiles + s - 1) / s;
+    const double cost = waves * (tps + 0.25) + 0.002 * s;  // last term: split reduction traffic
+    if (cost < best - 1e-9) {
+      best = cost;
+      best_s = s;
+    }
+  }
+  return best_s;
+}
+
+nbody_status ensure_partials(nbody_engine* e, int split) {
+  if (split <= e->p_splits) return NBODY_OK;
+  if (e->P) {
+    NB_CUDA(cudaStreamSynchronize(e->stream));
+    cudaFree(e->P);
+  }
+  if (e->graph) {  // the captured step refers to the old buffer
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  e->P = nullptr;
+  e->p_splits = 0;
+  NB_CUDA(cudaMalloc(&e->P, sizeof(double) * 6 * static_cast<size_t>(e->ld) * split));
+  e->p_splits = split;
+  return NBODY_OK;
+}
+
+nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_end,
+                         cudaStream_t st) {
+  const PairKernel& k = *t.k;
+  PairArgs a;
+  a.i_begin = i_begin;
+  a.i_end = i_end;
+  a.n_rows_pad = e->ld;
+  a.n_tiles = e->ld / k.tj;
+  a.tiles_per_split = (a.n_tiles + t.split - 1) / t.split;
+  a.eps2 = e->cfg.eps2;
+  a.out = e->P;
+  a.stride = static_cast<size_t>(e->ld);
+  a.status = e->status;
+  const int rows = i_end - i_begin;
+  if (rows <= 0) return NBODY_OK;
+  dim3 grid((rows + k.nt * k.ipt - 1) / (k.nt * k.ipt), t.split);
+  const void* jb = k.precision == NBODY_FP64 ? static_cast<const void*>(e->jb64)
+                                             : static_cast<const void*>(e->jb32);
+  void* args[] = {const_cast<void*>(static_cast<const void*>(&jb)), static_cast<void*>(&a)};
+  NB_CUDA(cudaLaunchKernel(k.fn, grid, dim3(k.nt), args, k.smem, st));
+  return NBODY_OK;
+}
+
+nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
+  const auto key = std::make_tuple(e->dev, e->cfg.precision, e->ld, rows);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      out->k = &registry()[it->second.first];
+      out->split = it->second.second;
+      return NBODY_OK;
+    }
+  }
+  cudaEvent_t a, b;
+  NB_CUDA(cudaEventCreate(&a));
+  NB_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_idx = -1, best_split = 1;
+  const auto& reg = registry();
+  for (size_t idx = 0; idx < reg.size(); ++idx) {
+    const PairKernel& k = reg[idx];
+    if (k.precision != e->cfg.precision) continue;
+    const int s0 = choose_split(e, k, rows);
+    for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
+      NB_TRY(ensure_partials(e, s));
+      Tiling t{&k, s};
+      NB_TRY(launch_pair(e, t, 0, rows, e->stream));  // warm-up
+      NB_CUDA(cudaEventRecord(a, e->stream));
+      for (int r = 0; r < 3; ++r) NB_TRY(launch_pair(e, t, 0, rows, e->stream));
+      NB_CUDA(cudaEventRecord(b, e->stream));
+      NB_CUDA(cudaEventSynchronize(b));
+      float ms = 0.f;
+      NB_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (ms < best) {
+        best = ms;
+        best_idx = static_cast<int>(idx);
+        best_split = s;
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  NB_TRY(check_status_word(e));
+  if (best_idx < 0) return fail(NBODY_ERR_STATE, "autotune found no kernel");
+  out->k = &reg[best_idx];
+  out->split = best_split;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tuned[key] = {best_idx, best_split};
+  return NBODY_OK;
+}
+
+// Tiling for `rows` i-rows: explicit config, else tuned, else heuristic.
+nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
+  const nbody_config& c = e->cfg;
+  const bool fp64 = c.precision == NBODY_FP64;
+  int nt = c.threads ? c.threads : 128;
+  int ipt = c.i_per_thread ? c.i_per_thread : (fp64 ? 2 : 4);
+  int tj = c.j_tile ? c.j_tile : 128;
+  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj);
+  if (!k)
+    return fail(NBODY_ERR_INVALID_ARG, "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d",
+                nt, ipt, tj);
+  if (c.tune && !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j)
+    return autotune(e, rows, out);
+  out->k = k;
+  out->split = c.split_j ? std::min(c.split_j, kMaxSplit) : choose_split(e, *k, rows);
+  return NBODY_OK;
+}
+
+nbody_status ensure_tiling(nbody_engine* e) {
+  if (e->tiled) return NBODY_OK;
+  NB_TRY(get_tiling(e, e->n, &e->tiling));
+  NB_TRY(ensure_partials(e, e->tiling.split));
+  e->tiled = true;
+  return NBODY_OK;
+}
+
+SoA7 own_inputs(nbody_engine* e) {
+  return SoA7{e->X, e->X + e->ld, e->X + 2 * e->ld, e->M, e->V, e->V + e->ld, e->V + 2 * e->ld};
+}
+SoA6 own_derivs(nbody_engine* e) {
+  double* D = e->D;
+  const size_t ld = e->ld;
+  return SoA6{D, D + ld, D + 2 * ld, D + 3 * ld, D + 4 * ld, D + 5 * ld};
+}
+
+nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
+  const bool fp64 = e->cfg.precision == NBODY_FP64;
+  // The FP64 records are always written: the potential reads them.
+  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(n, e->ld, in, e->jb64,
+                                                                      fp64 ? nullptr : e->jb32);
+  NB_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+// acc + jerk of the engine's current X, V, M into D (rows [0, n)).
+nbody_status eval_current(nbody_engine* e) {
+  NB_TRY(ensure_tiling(e));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  if (!e->init_events) {
+    NB_CUDA(cudaEventCreate(&e->ev_init[0]));
+    NB_CUDA(cudaEventCreate(&e->ev_init[1]));
+    e->init_events = true;
+  }
+  NB_CUDA(cudaEventRecord(e->ev_init[0], e->stream));
+  NB_TRY(launch_pair(e, e->tiling, 0, e->n, e->stream));
+  reduce_splits_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+      0, e->n, e->ld, e->tiling.split, e->P, own_derivs(e));
+  NB_CUDA(cudaGetLastError());
+  NB_CUDA(cudaEventRecord(e->ev_init[1], e->stream));
+  if (e->cfg.dt <= 0.0) {
+    initialdt_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+        e->n, e->ld, e->D, e->ctl, e->cfg.eta0);
+    NB_CUDA(cudaGetLastError());
+  }
+  e->have_derivs = true;
+  return NBODY_OK;
+}
+
+nbody_status enqueue_predict(nbody_engine* e, cudaStream_t st) {
+  const bool fp64 = e->cfg.precision == NBODY_FP64;
+  predict_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      e->n, e->ld, e->ctl, e->X, e->V, e->M, e->D, fp64 ? e->jb64 : nullptr,
+      fp64 ? nullptr : e->jb32);
+  NB_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+nbody_status enqueue_correct(nbody_engine* e, cudaStream_t st) {
+  correct_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      e->n, e->ld, e->tiling.split, e->P, e->X, e->V, e->D, e->ctl, e->cfg.eta);
+  NB_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+nbody_status build_step_graph(nbody_engine* e) {
+  if (e->graph) return NBODY_OK;
+  NB_TRY(ensure_tiling(e));
+  if (!e->step_events) {
+    for (auto& ev : e->ev) NB_CUDA(cudaEventCreate(&ev));
+    e->step_events = true;
+  }
+  cudaGraph_t g = nullptr;
+  NB_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  nbody_status s = NBODY_OK;
+  auto rec = [&](cudaEvent_t ev) {
+    if (s == NBODY_OK && cudaEventRecordWithFlags(ev, e->stream, cudaEventRecordExternal) != cudaSuccess)
+      s = fail(NBODY_ERR_CUDA, "event record during capture failed");
+  };
+  rec(e->ev[0]);
+  if (s == NBODY_OK) s = enqueue_predict(e, e->stream);
+  rec(e->ev[1]);
+  if (s == NBODY_OK) s = launch_pair(e, e->tiling, 0, e->n, e->stream);
+  rec(e->ev[2]);
+  if (s == NBODY_OK) s = enqueue_correct(e, e->stream);
+  rec(e->ev[3]);
+  cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+  if (s != NBODY_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (ce != cudaSuccess) return fail(NBODY_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    e->graph = nullptr;
+    return fail(NBODY_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+  }
+  return NBODY_OK;
+}
+
+nbody_status check_engine(nbody_engine* e) {
+  if (!e) return fail(NBODY_ERR_INVALID_ARG, "null engine");
+  if (cudaSetDevice(e->dev) != cudaSuccess) return fail(NBODY_ERR_CUDA, "cudaSetDevice(%d) failed", e->dev);
+  return NBODY_OK;
+}
+
+nbody_status need_state(nbody_engine* e) {
+  NB_TRY(check_engine(e));
+  if (!e->have_state) return fail(NBODY_ERR_STATE, "no state uploaded (call nbody_set_state)");
+  return NBODY_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* nbody_last_error(void) { return g_last_error.c_str(); }
+
+const char* nbody_status_string(nbody_status s) {
+  switch (s) {
+    case NBODY_OK: return "ok";
+    case NBODY_ERR_INVALID_ARG: return "invalid argument";
+    case NBODY_ERR_OOM: return "out of memory";
+    case NBODY_ERR_CUDA: return "CUDA error";
+    case NBODY_ERR_TIMEOUT: return "in-kernel wait timed out";
+    case NBODY_ERR_NONFINITE: return "non-finite value";
+    case NBODY_ERR_NO_DEVICE: return "no usable device";
+    case NBODY_ERR_STATE: return "call order";
+  }
+  return "unknown status";
+}
+
+nbody_status nbody_config_init(nbody_config* c) {
+  if (!c) return fail(NBODY_ERR_INVALID_ARG, "null config");
+  memset(c, 0, sizeof *c);
+  c->n = 0;
+  c->eps2 = 1.0e-7;
+  c->precision = NBODY_FP64;
+  c->device = 0;
+  c->dt = 0.0;
+  c->eta = 1.0e-2;
+  c->eta0 = 1.0e-4;
+  return NBODY_OK;
+}
+
+nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
+  if (!out || !cfg) return fail(NBODY_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->n < 1 || cfg->n > (1 << 28)) return fail(NBODY_ERR_INVALID_ARG, "n = %d out of range", cfg->n);
+  if (!(cfg->eps2 >= 1e-30 && cfg->eps2 <= 1e30))
+    return fail(NBODY_ERR_INVALID_ARG, "eps2 = %g outside [1e-30, 1e30]", cfg->eps2);
+  if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
+    return fail(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
+  if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
+  if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
+    return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(NBODY_ERR_NO_DEVICE, "no CUDA device visible");
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return fail(NBODY_ERR_INVALID_ARG, "device %d of %d", cfg->device, ndev);
+  cudaDeviceProp prop;
+  NB_CUDA(cudaGetDeviceProperties(&prop, cfg->device));
+  if (prop.major != 10)
+    return fail(NBODY_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
+                cfg->device, prop.major, prop.minor);
+  NB_CUDA(cudaSetDevice(cfg->device));
+
+  std::unique_ptr<nbody_engine> e(new nbody_engine);
+  e->cfg = *cfg;
+  e->n = cfg->n;
+  e->ld = round_up(cfg->n, kPad);
+  e->dev = cfg->device;
+  e->num_sms = prop.multiProcessorCount;
+  const size_t ld = e->ld;
+  auto cleanup_on_fail = [&](nbody_status s) {
+    nbody_destroy(e.release());
+    return s;
+  };
+  nbody_status s = [&]() -> nbody_status {
+    NB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    NB_CUDA(cudaMalloc(&e->state, sizeof(double) * 13 * ld));
+    NB_CUDA(cudaMemsetAsync(e->state, 0, sizeof(double) * 13 * ld, e->stream));
+    e->X = e->state;
+    e->V = e->state + 3 * ld;
+    e->M = e->state + 6 * ld;
+    e->D = e->state + 7 * ld;
+    NB_CUDA(cudaMalloc(&e->jb64, sizeof(JBody64) * ld));
+    if (cfg->precision == NBODY_MIXED) NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBody32) * ld));
+    NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
+    NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 + 8)));
+    NB_CUDA(cudaMalloc(&e->status, sizeof(int)));
+    NB_CUDA(cudaMemsetAsync(e->status, 0, sizeof(int), e->stream));
+    NB_CUDA(cudaStreamSynchronize(e->stream));
+    return NBODY_OK;
+  }();
+  if (s != NBODY_OK) return cleanup_on_fail(s);
+  *out = e.release();
+  return NBODY_OK;
+}
+
+nbody_status nbody_destroy(nbody_engine* e) {
+  if (!e) return NBODY_OK;
+  cudaSetDevice(e->dev);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (auto ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto ev : e->ev_init)
+    if (ev) cudaEventDestroy(ev);
+  cudaFree(e->state);
+  cudaFree(e->P);
+  cudaFree(e->jb64);
+  cudaFree(e->jb32);
+  cudaFree(e->ctl);
+  cudaFree(e->partial);
+  cudaFree(e->status);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return NBODY_OK;
+}
+
+nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, const double* z,
+                             const double* m, const double* vx, const double* vy,
+                             const double* vz) {
+  NB_TRY(check_engine(e));
+  const double* src[7] = {x, y, z, vx, vy, vz, m};
+  for (auto p : src)
+    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null state array");
+  const size_t ld = e->ld, b = sizeof(double) * e->n;
+  double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};
+  for (int k = 0; k < 7; ++k)
+    NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
+  StepCtl c{};
+  c.dt = e->cfg.dt > 0 ? e->cfg.dt : 0.0;
+  c.t = 0.0;
+  c.dt_crit = 0.0;
+  c.crit_bits = kPosInfBits;
+  c.blocks_done = 0;
+  c.adaptive = e->cfg.dt > 0 ? 0 : 1;
+  c.steps = 0;
+  NB_CUDA(cudaMemcpyAsync(e->ctl, &c, sizeof c, cudaMemcpyHostToDevice, e->stream));
+  NB_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * ld, e->stream));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  e->have_state = true;
+  e->have_derivs = false;
+  return NBODY_OK;
+}
+
+nbody_status nbody_get_state(nbody_engine* e, double* x, double* y, double* z, double* vx,
+                             double* vy, double* vz) {
+  NB_TRY(need_state(e));
+  const size_t ld = e->ld, b = sizeof(double) * e->n;
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  const double* src[6] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyDeviceToHost, e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return check_status_word(e);
+}
+
+nbody_status nbody_get_derivs(nbody_engine* e, double* ax, double* ay, double* az, double* jx,
+                              double* jy, double* jz) {
+  NB_TRY(need_state(e));
+  if (!e->have_derivs) return fail(NBODY_ERR_STATE, "no derivatives yet (call nbody_acc_jerk)");
+  const size_t ld = e->ld, b = sizeof(double) * e->n;
+  double* dst[6] = {ax, ay, az, jx, jy, jz};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) NB_CUDA(cudaMemcpyAsync(dst[k], e->D + k * ld, b, cudaMemcpyDeviceToHost, e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return check_status_word(e);
+}
+
+nbody_status nbody_acc_jerk(nbody_engine* e) {
+  NB_TRY(need_state(e));
+  return eval_current(e);
+}
+
+nbody_status nbody_predict(nbody_engine* e) {
+  NB_TRY(need_state(e));
+  if (!e->have_derivs) NB_TRY(eval_current(e));
+  return enqueue_predict(e, e->stream);
+}
+
+nbody_status nbody_eval_predicted(nbody_engine* e) {
+  NB_TRY(need_state(e));
+  NB_TRY(ensure_tiling(e));
+  return launch_pair(e, e->tiling, 0, e->n, e->stream);
+}
+
+nbody_status nbody_correct(nbody_engine* e) {
+  NB_TRY(need_state(e));
+  NB_TRY(ensure_tiling(e));
+  return enqueue_correct(e, e->stream);
+}
+
+nbody_status nbody_step(nbody_engine* e, int nsteps) {
+  NB_TRY(need_state(e));
+  if (nsteps < 0) return fail(NBODY_ERR_INVALID_ARG, "nsteps < 0");
+  if (!e->have_derivs) NB_TRY(eval_current(e));
+  NB_TRY(build_step_graph(e));
+  for (int k = 0; k < nsteps; ++k) NB_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  return NBODY_OK;
+}
+
+nbody_status nbody_synchronize(nbody_engine* e) {
+  NB_TRY(check_engine(e));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return check_status_word(e);
+}
+
+nbody_status nbody_energy(nbody_engine* e, int ref_compat, double* T, double* U) {
+  NB_TRY(need_state(e));
+  const int nb = e->ld / kBlockO1;
+  double* scal = e->partial + nb;  // two result slots after the partials
+  kinetic_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->V, e->M, e->partial);
+  sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal);
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  potential_kernel<kBlockO1><<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->cfg.eps2,
+                                                             ref_compat ? 1 : 0, e->jb64, e->partial);
+  sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal + 1);
+  NB_CUDA(cudaGetLastError());
+  double h[2];
+  NB_CUDA(cudaMemcpyAsync(h, scal, sizeof h, cudaMemcpyDeviceToHost, e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  const double t = h[0];
+  const double u = ref_compat ? -h[1] : -0.5 * h[1];
+  if (T) *T = t;
+  if (U) *U = u;
+  if (!std::isfinite(t) || !std::isfinite(u))
+    return fail(NBODY_ERR_NONFINITE, "energy is not finite (T=%g U=%g)", t, u);
+  return NBODY_OK;
+}
+
+nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
+  NB_TRY(check_engine(e));
+  if (!out) return fail(NBODY_ERR_INVALID_ARG, "null timers");
+  memset(out, 0, sizeof *out);
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  float ms = 0.f;
+  if (e->step_events && e->graph) {
+    if (cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]) == cudaSuccess) out->pred_ms = ms;
+    if (cudaEventElapsedTime(&ms, e->ev[1], e->ev[2]) == cudaSuccess) out->eval_ms = ms;
+    if (cudaEventElapsedTime(&ms, e->ev[2], e->ev[3]) == cudaSuccess) out->corr_ms = ms;
+    cudaGetLastError();
+  }
+  if (e->init_events && cudaEventElapsedTime(&ms, e->ev_init[0], e->ev_init[1]) == cudaSuccess)
+    out->eval_init_ms = ms;
+  cudaGetLastError();
+  out->num_sms = e->num_sms;
+  if (e->tiled) {
+    out->threads = e->tiling.k->nt;
+    out->i_per_thread = e->tiling.k->ipt;
+    out->j_tile = e->tiling.k->tj;
+    out->split_j = e->tiling.split;
+  }
+  if (e->have_state) {
+    StepCtl c;
+    NB_CUDA(cudaMemcpy(&c, e->ctl, sizeof c, cudaMemcpyDeviceToHost));
+    out->steps = c.steps;
+    out->t = c.t;
+    out->dt = c.dt;
+  }
+  return NBODY_OK;
+}
+
+nbody_status nbody_get_stream(nbody_engine* e, void** stream) {
+  NB_TRY(check_engine(e));
+  if (!stream) return fail(NBODY_ERR_INVALID_ARG, "null stream out");
+  *stream = e->stream;
+  return NBODY_OK;
+}
+
+nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, const double* y,
+                                   const double* z, const double* m, const double* vx,
+                                   const double* vy, const double* vz, double* ax, double* ay,
+                                   double* az, double* jx, double* jy, double* jz, void* stream) {
+  NB_TRY(check_engine(e));
+  if (n < 1 || n > e->n) return fail(NBODY_ERR_INVALID_ARG, "n = %d outside [1, %d]", n, e->n);
+  const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
+  for (auto p : ptrs)
+    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null device array");
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : e->stream;
+  Tiling t;
+  NB_TRY(get_tiling(e, n, &t));
+  NB_TRY(ensure_partials(e, t.split));
+  NB_TRY(launch_pack(e, n, SoA7{x, y, z, m, vx, vy, vz}, st));
+  NB_TRY(launch_pair(e, t, 0, n, st));
+  reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      0, n, e->ld, t.split, e->P, SoA6{ax, ay, az, jx, jy, jz});
+  NB_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Drop-in force_calculation: cached engines per (thread, device, precision).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DropIn {
+  nbody_engine* e = nullptr;
+  int n = 0;
+  double eps2 = 0;
+};
+
+struct DropInCache {
+  std::map<std::pair<int, int>, DropIn> m;
+  ~DropInCache() {
+    for (auto& kv : m) nbody_destroy(kv.second.e);
+  }
+};
+thread_local DropInCache g_dropin;
+
+}  // namespace
+
+extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin,
+                                                int i_end, const double* x, const double* y,
+                                                const double* z, const double* m,
+                                                const double* vx, const double* vy,
+                                                const double* vz, double* ax, double* ay,
+                                                double* az, double* jx, double* jy, double* jz) {
+  if (n < 1) return fail(NBODY_ERR_INVALID_ARG, "n = %d", n);
+  if (i_begin < 0 || i_end > n || i_begin > i_end)
+    return fail(NBODY_ERR_INVALID_ARG, "row range [%d, %d) outside [0, %d)", i_begin, i_end, n);
+  const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
+  for (auto p : ptrs)
+    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null array");
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  DropIn& d = g_dropin.m[{dev, precision}];
+  if (!d.e || d.n != n || d.eps2 != eps2) {
+    nbody_destroy(d.e);
+    d.e = nullptr;
+    nbody_config c;
+    nbody_config_init(&c);
+    c.n = n;
+    c.eps2 = eps2;
+    c.precision = precision;
+    c.device = dev;
+    c.dt = 1.0;  // fixed: no initial-dt pass on the drop-in path
+    NB_TRY(nbody_create(&d.e, &c));
+    d.n = n;
+    d.eps2 = eps2;
+  }
+  nbody_engine* e = d.e;
+  const size_t ld = e->ld, b = sizeof(double) * n;
+  const double* src[7] = {x, y, z, vx, vy, vz, m};
+  double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};
+  for (int k = 0; k < 7; ++k)
+    NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
+  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream));
+  NB_TRY(ensure_tiling(e));
+  Tiling t = e->tiling;
+  if (i_end - i_begin != n) NB_TRY(get_tiling(e, i_end - i_begin, &t));
+  NB_TRY(ensure_partials(e, t.split));
+  NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
+  if (i_end > i_begin) {
+    reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+        i_begin, i_end, e->ld, t.split, e->P, own_derivs(e));
+    NB_CUDA(cudaGetLastError());
+  }
+  double* out[6] = {ax, ay, az, jx, jy, jz};
+  const size_t rb = sizeof(double) * (i_end - i_begin);
+  for (int k = 0; k < 6; ++k) {
+    if (i_begin > 0) memset(out[k], 0, sizeof(double) * i_begin);
+    if (i_end < n) memset(out[k] + i_end, 0, sizeof(double) * (n - i_end));
+    if (rb) NB_CUDA(cudaMemcpyAsync(out[k] + i_begin, e->D + k * ld + i_begin, rb,
+                                    cudaMemcpyDeviceToHost, e->stream));
+  }
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return check_status_word(e);
+}
+
+extern "C" nbody_status nbody_force_calculation_release(void) {
+  for (auto& kv : g_dropin.m) nbody_destroy(kv.second.e);
+  g_dropin.m.clear();
+  return NBODY_OK;
+}
