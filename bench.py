@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--tune", action="store_true", help="autotune pair-kernel tiling first")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the main arm only (no peaks, e2e, CPU baseline): the profiling case")
     return ap.parse_args()
 
 
@@ -77,7 +79,7 @@ class ClockSampler:
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.p = None
@@ -317,6 +319,13 @@ def main():
     torch.cuda.set_device(dev)
     import nbody_b200 as nb
     state = nb.plummer(a.n, a.seed)
+    if a.kernels_only:
+        arm = run_arm(a, a.precision, state, torch, dist, rank, world, dev)
+        if rank == 0:
+            print(json.dumps({"kernels_only": True, "precision": a.precision, "n": a.n, **arm}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     peaks = nb.measure_peaks(dev)
     main_arm = run_arm(a, a.precision, state, torch, dist, rank, world, dev)
     other = None
