@@ -157,6 +157,26 @@ nbody_status nbody_acc_jerk_device(nbody_engine* eng, int n, const double* x, co
                                    double* az, double* jx, double* jy, double* jz,
                                    void* stream);
 
+/* ---- allocation-free variant of nbody_acc_jerk_device ----------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory (an application that owns the device memory budget through
+ * its own pool, a real-time loop where cudaMalloc/cudaFree would stall the
+ * device, code running inside someone else's time-step loop): same inputs,
+ * outputs and physics as nbody_acc_jerk_device, but no engine and no
+ * cudaMalloc - its scratch is a 16 MiB static device array inside the
+ * library, held by every GPU that loads the library until the process exits.
+ * n must be <= 32768 (NBODY_ERR_INVALID_ARG beyond).  Arrays are float64 on
+ * the current device; work is enqueued on `stream` (cudaStream_t, NULL = the
+ * legacy default stream) and the call returns without waiting.  The first
+ * call on a device looks up the scratch address (cudaGetSymbolAddress); make
+ * it before any stream capture.  All calls share the scratch: calls that
+ * overlap on the GPU race; order them on one stream. */
+nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision, const double* x,
+                                    const double* y, const double* z, const double* m,
+                                    const double* vx, const double* vy, const double* vz,
+                                    double* ax, double* ay, double* az, double* jx, double* jy,
+                                    double* jz, void* stream);
+
 /* ---- initial conditions (host, deterministic) ------------------------------
  * Plummer sphere in Henon units (G = M = 1, E = -1/4), equal masses 1/n,
  * centred on the origin in position and velocity; sampled by the

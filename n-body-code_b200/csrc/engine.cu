@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/nbody_cuda.h"
+#include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
 
@@ -114,6 +115,16 @@ std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;  // -> (kernel idx, split)
 
 }  // namespace
+
+nbody_status nbody_set_error(nbody_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
 
 struct nbody_engine {
   nbody_config cfg{};

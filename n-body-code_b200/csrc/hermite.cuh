@@ -119,7 +119,7 @@ struct SoA6 {
 
 // Writes j-records for rows [0, ld): rows < n from `in`, the rest as
 // zero-mass bodies at rest at the origin (they contribute exactly zero).
-__global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__ jb64,
+static __global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__ jb64,
                             JBody32* __restrict__ jb32) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ld) return;
@@ -139,7 +139,7 @@ __global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__ jb64,
 
 // Predictor: in place on X, V (rows < n) and writes the j-records of the
 // predicted state (jb64 or jb32, whichever is non-null).
-__global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__ ctl, double* __restrict__ X,
+static __global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__ ctl, double* __restrict__ X,
                                double* __restrict__ V, const double* __restrict__ M,
                                const double* __restrict__ D, JBody64* __restrict__ jb64,
                                JBody32* __restrict__ jb32) {
@@ -170,7 +170,7 @@ __global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__ ctl, d
 
 // Corrector fused with the split-j reduction and the Aarseth criterion:
 // a1/j1 = sum over S splits of P; snap/crackle; correct X, V; D <- a1/j1.
-__global__ void correct_kernel(int n, int ld, int S, const double* __restrict__ P,
+static __global__ void correct_kernel(int n, int ld, int S, const double* __restrict__ P,
                                double* __restrict__ X, double* __restrict__ V,
                                double* __restrict__ D, StepCtl* __restrict__ ctl, double eta) {
   __shared__ double sh[32];
@@ -207,7 +207,7 @@ __global__ void correct_kernel(int n, int ld, int S, const double* __restrict__ 
 }
 
 // out[c][i] = sum_s P[s][c][i] for rows [i_begin, i_end), splits in order.
-__global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int S,
+static __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int S,
                                      const double* __restrict__ P, SoA6 out) {
   const int i = i_begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= i_end) return;
@@ -221,7 +221,7 @@ __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int S,
 }
 
 // Initial step criterion min_i eta0 |a| / |j| (published via ctl).
-__global__ void initialdt_kernel(int n, int ld, const double* __restrict__ D, StepCtl* ctl,
+static __global__ void initialdt_kernel(int n, int ld, const double* __restrict__ D, StepCtl* ctl,
                                  double eta0) {
   __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -235,7 +235,7 @@ __global__ void initialdt_kernel(int n, int ld, const double* __restrict__ D, St
 }
 
 // Per-CTA partial of 0.5 m v^2.
-__global__ void kinetic_kernel(int n, int ld, const double* __restrict__ V,
+static __global__ void kinetic_kernel(int n, int ld, const double* __restrict__ V,
                                const double* __restrict__ M, double* __restrict__ partial) {
   __shared__ double sh[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -254,7 +254,7 @@ __global__ void kinetic_kernel(int n, int ld, const double* __restrict__ V,
 // regrouped by j; CTA partial of m_i^2 psi_i).  FP64, j-tiles staged
 // through shared memory by the CTA's threads.
 template <int NT>
-__global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, double eps2, int mode,
+static __global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, double eps2, int mode,
                                                        const JBody64* __restrict__ jb,
                                                        double* __restrict__ partial) {
   __shared__ double4 tile[NT];
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, double eps
 }
 
 // Sums `count` partials in a fixed order (one CTA).
-__global__ void sum_partials_kernel(int count, const double* __restrict__ partial,
+static __global__ void sum_partials_kernel(int count, const double* __restrict__ partial,
                                     double* __restrict__ out) {
   __shared__ double sh[32];
   double v = 0.0;
