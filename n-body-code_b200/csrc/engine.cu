@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -70,37 +71,49 @@ nbody_status fail(nbody_status s, const char* fmt, ...) {
 // ---------------------------------------------------------------------------
 struct PairKernel {
   int precision, nt, ipt, tj;
+  int fmt;      // RecordFormat of the j-records it reads
   const void* fn;
   size_t smem;  // dynamic shared memory: two j-tile buffers
-  size_t rec;   // bytes per j-record
 };
 
 template <int NT, int IPT, int TJ>
 PairKernel make_fp64() {
-  return {NBODY_FP64, NT, IPT, TJ, reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ>),
-          2 * TJ * sizeof(JBody64), sizeof(JBody64)};
+  return {NBODY_FP64, NT, IPT, TJ, kRecF64,
+          reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBody64)};
 }
 template <int NT, int IPT, int TJ>
 PairKernel make_mixed() {
-  return {NBODY_MIXED, NT, IPT, TJ, reinterpret_cast<const void*>(&pair_mixed_kernel<NT, IPT, TJ>),
-          2 * TJ * sizeof(JBody32), sizeof(JBody32)};
+  return {NBODY_MIXED, NT, IPT, TJ, kRecF32,
+          reinterpret_cast<const void*>(&pair_mixed_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBody32)};
+}
+template <int NT, int IPT, int TJ>
+PairKernel make_mixed_x2() {
+  return {NBODY_MIXED, NT, IPT, TJ, kRecX2,
+          reinterpret_cast<const void*>(&pair_mixed_x2_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBodyX2)};
 }
 
+// The first entry of each precision is its default; packed-pair (x2) kernels
+// are preferred over scalar ones of the same shape.
 const std::vector<PairKernel>& registry() {
   static const std::vector<PairKernel> r = {
-      make_fp64<128, 1, 128>(),  make_fp64<128, 2, 128>(),  make_fp64<128, 4, 128>(),
-      make_fp64<256, 1, 128>(),  make_fp64<256, 2, 128>(),  make_fp64<128, 2, 256>(),
-      make_fp64<64, 2, 128>(),   make_fp64<64, 4, 128>(),
-      make_mixed<128, 1, 128>(), make_mixed<128, 2, 128>(), make_mixed<128, 4, 128>(),
-      make_mixed<256, 2, 128>(), make_mixed<128, 4, 256>(), make_mixed<256, 4, 256>(),
-      make_mixed<64, 4, 128>(),  make_mixed<128, 2, 256>(),
+      make_fp64<128, 2, 128>(),     make_fp64<128, 1, 128>(),     make_fp64<128, 4, 128>(),
+      make_fp64<256, 1, 128>(),     make_fp64<256, 2, 128>(),     make_fp64<128, 2, 256>(),
+      make_fp64<64, 2, 128>(),      make_fp64<64, 4, 128>(),
+      make_mixed_x2<128, 4, 128>(), make_mixed_x2<128, 2, 128>(), make_mixed_x2<256, 2, 128>(),
+      make_mixed_x2<256, 4, 128>(), make_mixed_x2<64, 4, 128>(),  make_mixed_x2<128, 4, 64>(),
+      make_mixed<128, 4, 128>(),    make_mixed<128, 2, 128>(),    make_mixed<256, 2, 128>(),
+      make_mixed<128, 4, 256>(),    make_mixed<64, 4, 128>(),
   };
   return r;
 }
 
-const PairKernel* find_kernel(int precision, int nt, int ipt, int tj) {
+// variant (mixed only): 0 = packed-pair kernel when one of that shape
+// exists, 1 = scalar kernel.
+const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
   for (const auto& k : registry())
-    if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj) return &k;
+    if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj &&
+        (precision == NBODY_FP64 || (variant == 1) == (k.fmt == kRecF32)))
+      return &k;
   return nullptr;
 }
 
@@ -135,7 +148,7 @@ struct nbody_engine {
   double* P = nullptr;
   int p_splits = 0;
   JBody64* jb64 = nullptr;
-  JBody32* jb32 = nullptr;
+  void* jb32 = nullptr;  // mixed records: JBody32 or JBodyX2 (sized for the larger)
   StepCtl* ctl = nullptr;
   double* partial = nullptr;  // reduction scratch: ld / 256 + 1 doubles + 4 scalars
   int* status = nullptr;
@@ -221,12 +234,15 @@ nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_en
   const int rows = i_end - i_begin;
   if (rows <= 0) return NBODY_OK;
   dim3 grid((rows + k.nt * k.ipt - 1) / (k.nt * k.ipt), t.split);
-  const void* jb = k.precision == NBODY_FP64 ? static_cast<const void*>(e->jb64)
-                                             : static_cast<const void*>(e->jb32);
+  const void* jb = k.fmt == kRecF64 ? static_cast<const void*>(e->jb64)
+                                     : static_cast<const void*>(e->jb32);
   void* args[] = {const_cast<void*>(static_cast<const void*>(&jb)), static_cast<void*>(&a)};
   NB_CUDA(cudaLaunchKernel(k.fn, grid, dim3(k.nt), args, k.smem, st));
   return NBODY_OK;
 }
+
+SoA7 own_inputs(nbody_engine* e);
+nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt);
 
 nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   const auto key = std::make_tuple(e->dev, e->cfg.precision, e->ld, rows);
@@ -249,6 +265,7 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
     const PairKernel& k = reg[idx];
     if (k.precision != e->cfg.precision) continue;
     const int s0 = choose_split(e, k, rows);
+    NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt));
     for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
       NB_TRY(ensure_partials(e, s));
       Tiling t{&k, s};
@@ -259,6 +276,9 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
       NB_CUDA(cudaEventSynchronize(b));
       float ms = 0.f;
       NB_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (getenv("NBODY_TUNE_VERBOSE"))
+        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d split=%d  %.4f ms\n",
+                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, s, ms / 3);
       if (ms < best) {
         best = ms;
         best_idx = static_cast<int>(idx);
@@ -284,11 +304,12 @@ nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
   int nt = c.threads ? c.threads : 128;
   int ipt = c.i_per_thread ? c.i_per_thread : (fp64 ? 2 : 4);
   int tj = c.j_tile ? c.j_tile : 128;
-  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj);
+  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, c.pair_variant);
   if (!k)
-    return fail(NBODY_ERR_INVALID_ARG, "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d",
-                nt, ipt, tj);
-  if (c.tune && !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j)
+    return fail(NBODY_ERR_INVALID_ARG,
+                "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d variant=%d", nt,
+                ipt, tj, c.pair_variant);
+  if (c.tune && !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j && !c.pair_variant)
     return autotune(e, rows, out);
   out->k = k;
   out->split = c.split_j ? std::min(c.split_j, kMaxSplit) : choose_split(e, *k, rows);
@@ -312,19 +333,22 @@ SoA6 own_derivs(nbody_engine* e) {
   return SoA6{D, D + ld, D + 2 * ld, D + 3 * ld, D + 4 * ld, D + 5 * ld};
 }
 
-nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
-  const bool fp64 = e->cfg.precision == NBODY_FP64;
-  // The FP64 records are always written: the potential reads them.
-  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(n, e->ld, in, e->jb64,
-                                                                      fp64 ? nullptr : e->jb32);
+// Writes the FP64 records (always: the potential reads them) and, for a
+// mixed kernel, the records in that kernel's format.
+nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt) {
+  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      n, e->ld, in, e->jb64, fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
+      fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
 
+int tiling_fmt(const nbody_engine* e) { return e->tiled ? e->tiling.k->fmt : kRecF64; }
+
 // acc + jerk of the engine's current X, V, M into D (rows [0, n)).
 nbody_status eval_current(nbody_engine* e) {
   NB_TRY(ensure_tiling(e));
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e)));
   if (!e->init_events) {
     NB_CUDA(cudaEventCreate(&e->ev_init[0]));
     NB_CUDA(cudaEventCreate(&e->ev_init[1]));
@@ -346,10 +370,11 @@ nbody_status eval_current(nbody_engine* e) {
 }
 
 nbody_status enqueue_predict(nbody_engine* e, cudaStream_t st) {
-  const bool fp64 = e->cfg.precision == NBODY_FP64;
+  const int fmt = tiling_fmt(e);
   predict_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      e->n, e->ld, e->ctl, e->X, e->V, e->M, e->D, fp64 ? e->jb64 : nullptr,
-      fp64 ? nullptr : e->jb32);
+      e->n, e->ld, e->ctl, e->X, e->V, e->M, e->D, fmt == kRecF64 ? e->jb64 : nullptr,
+      fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
+      fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
@@ -456,6 +481,8 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
   if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
+  if (cfg->pair_variant != 0 && cfg->pair_variant != 1)
+    return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(NBODY_ERR_NO_DEVICE, "no CUDA device visible");
@@ -488,7 +515,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
     e->M = e->state + 6 * ld;
     e->D = e->state + 7 * ld;
     NB_CUDA(cudaMalloc(&e->jb64, sizeof(JBody64) * ld));
-    if (cfg->precision == NBODY_MIXED) NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBody32) * ld));
+    if (cfg->precision == NBODY_MIXED) NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyX2) * ld));
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
     NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 + 8)));
     NB_CUDA(cudaMalloc(&e->status, sizeof(int)));
@@ -543,7 +570,7 @@ nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, 
   c.steps = 0;
   NB_CUDA(cudaMemcpyAsync(e->ctl, &c, sizeof c, cudaMemcpyHostToDevice, e->stream));
   NB_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * ld, e->stream));
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e)));
   NB_CUDA(cudaStreamSynchronize(e->stream));
   e->have_state = true;
   e->have_derivs = false;
@@ -618,7 +645,7 @@ nbody_status nbody_energy(nbody_engine* e, int ref_compat, double* T, double* U)
   double* scal = e->partial + nb;  // two result slots after the partials
   kinetic_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->V, e->M, e->partial);
   sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal);
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, kRecF64));
   potential_kernel<kBlockO1><<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->cfg.eps2,
                                                              ref_compat ? 1 : 0, e->jb64, e->partial);
   sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal + 1);
@@ -687,7 +714,7 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   Tiling t;
   NB_TRY(get_tiling(e, n, &t));
   NB_TRY(ensure_partials(e, t.split));
-  NB_TRY(launch_pack(e, n, SoA7{x, y, z, m, vx, vy, vz}, st));
+  NB_TRY(launch_pack(e, n, SoA7{x, y, z, m, vx, vy, vz}, st, t.k->fmt));
   NB_TRY(launch_pair(e, t, 0, n, st));
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
       0, n, e->ld, t.split, e->P, SoA6{ax, ay, az, jx, jy, jz});
@@ -753,11 +780,11 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};
   for (int k = 0; k < 7; ++k)
     NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
-  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream));
   NB_TRY(ensure_tiling(e));
   Tiling t = e->tiling;
   if (i_end - i_begin != n) NB_TRY(get_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
+  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt));
   NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
   if (i_end > i_begin) {
     reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(

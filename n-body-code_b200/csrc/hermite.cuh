@@ -108,6 +108,21 @@ __device__ __forceinline__ JBody32 make_jb32(double x, double y, double z, doubl
   return b;
 }
 
+__device__ __forceinline__ JBodyX2 make_jbx2(double x, double y, double z, double m, double vx,
+                                             double vy, double vz) {
+  const JBody32 b = make_jb32(x, y, z, m, vx, vy, vz);
+  JBodyX2 d;
+  d.xh = make_float2(b.xh, b.xh); d.yh = make_float2(b.yh, b.yh); d.zh = make_float2(b.zh, b.zh);
+  d.m = make_float2(b.m, b.m);
+  d.xl = make_float2(b.xl, b.xl); d.yl = make_float2(b.yl, b.yl); d.zl = make_float2(b.zl, b.zl);
+  d.vx = make_float2(b.vx, b.vx); d.vy = make_float2(b.vy, b.vy); d.vz = make_float2(b.vz, b.vz);
+  d.pad0 = d.pad1 = make_float2(0.f, 0.f);
+  return d;
+}
+
+// j-record formats of the pair kernels.
+enum RecordFormat { kRecF64 = 0, kRecF32 = 1, kRecX2 = 2 };
+
 // Seven SoA input arrays (caller's or the engine's own).
 struct SoA7 {
   const double *x, *y, *z, *m, *vx, *vy, *vz;
@@ -120,7 +135,7 @@ struct SoA6 {
 // Writes j-records for rows [0, ld): rows < n from `in`, the rest as
 // zero-mass bodies at rest at the origin (they contribute exactly zero).
 static __global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__ jb64,
-                            JBody32* __restrict__ jb32) {
+                            JBody32* __restrict__ jb32, JBodyX2* __restrict__ jbx2 = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ld) return;
   double x = 0, y = 0, z = 0, m = 0, vx = 0, vy = 0, vz = 0;
@@ -135,6 +150,7 @@ static __global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__
     jb64[i] = b;
   }
   if (jb32) jb32[i] = make_jb32(x, y, z, m, vx, vy, vz);
+  if (jbx2) jbx2[i] = make_jbx2(x, y, z, m, vx, vy, vz);
 }
 
 // Predictor: in place on X, V (rows < n) and writes the j-records of the
@@ -142,7 +158,7 @@ static __global__ void pack_kernel(int n, int ld, SoA7 in, JBody64* __restrict__
 static __global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__ ctl, double* __restrict__ X,
                                double* __restrict__ V, const double* __restrict__ M,
                                const double* __restrict__ D, JBody64* __restrict__ jb64,
-                               JBody32* __restrict__ jb32) {
+                               JBody32* __restrict__ jb32, JBodyX2* __restrict__ jbx2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double dt = ctl->dt;
@@ -166,6 +182,7 @@ static __global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__
     jb64[i] = b;
   }
   if (jb32) jb32[i] = make_jb32(p[0], p[1], p[2], m, u[0], u[1], u[2]);
+  if (jbx2) jbx2[i] = make_jbx2(p[0], p[1], p[2], m, u[0], u[1], u[2]);
 }
 
 // Corrector fused with the split-j reduction and the Aarseth criterion:

@@ -58,7 +58,8 @@ DeviceSetup g_dev[kMaxDevices];
 
 constexpr int kIptFp64 = 2, kIptMixed = 4;
 const void* kernel_fp64() { return reinterpret_cast<const void*>(&pair_fp64_kernel<kThreads, kIptFp64, kTile>); }
-const void* kernel_mixed() { return reinterpret_cast<const void*>(&pair_mixed_kernel<kThreads, kIptMixed, kTile>); }
+// the engine's default mixed kernel (packed pairs), so both entry points do identical arithmetic
+const void* kernel_mixed() { return reinterpret_cast<const void*>(&pair_mixed_x2_kernel<kThreads, kIptMixed, kTile>); }
 
 nbody_status setup(int dev, DeviceSetup** out) {
   std::lock_guard<std::mutex> g(g_mu);
@@ -78,7 +79,7 @@ nbody_status setup(int dev, DeviceSetup** out) {
         d.occ_fp64 < 1)
       d.occ_fp64 = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_mixed, kernel_mixed(), kThreads,
-                                                      2 * kTile * sizeof(JBody32)) != cudaSuccess ||
+                                                      2 * kTile * sizeof(JBodyX2)) != cudaSuccess ||
         d.occ_mixed < 1)
       d.occ_mixed = 1;
     cudaGetLastError();
@@ -118,7 +119,7 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
 
   const bool fp64 = precision == NBODY_FP64;
   const int ld = (n + kPadRows - 1) / kPadRows * kPadRows;
-  const size_t rec = fp64 ? sizeof(JBody64) : sizeof(JBody32);
+  const size_t rec = fp64 ? sizeof(JBody64) : sizeof(JBodyX2);
   const size_t jb_bytes = (static_cast<size_t>(ld) * rec + 255) / 256 * 256;
   const size_t split_bytes = sizeof(double) * 6 * static_cast<size_t>(ld);
   const int cap = static_cast<int>((kScratchBytes - kStatusBytes - jb_bytes) / split_bytes);
@@ -146,8 +147,8 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
   if (cudaMemsetAsync(status, 0, sizeof(int), cs) != cudaSuccess)
     return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: clearing the status word failed");
   pack_kernel<<<(ld + 255) / 256, 256, 0, cs>>>(
-      n, ld, SoA7{x, y, z, m, vx, vy, vz}, fp64 ? reinterpret_cast<JBody64*>(jb) : nullptr,
-      fp64 ? nullptr : reinterpret_cast<JBody32*>(jb));
+      n, ld, SoA7{x, y, z, m, vx, vy, vz}, fp64 ? reinterpret_cast<JBody64*>(jb) : nullptr, nullptr,
+      fp64 ? nullptr : reinterpret_cast<JBodyX2*>(jb));
   PairArgs a;
   a.i_begin = 0;
   a.i_end = n;
@@ -163,8 +164,8 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
     pair_fp64_kernel<kThreads, kIptFp64, kTile><<<grid, kThreads, 2 * kTile * sizeof(JBody64), cs>>>(
         reinterpret_cast<const JBody64*>(jb), a);
   else
-    pair_mixed_kernel<kThreads, kIptMixed, kTile><<<grid, kThreads, 2 * kTile * sizeof(JBody32), cs>>>(
-        reinterpret_cast<const JBody32*>(jb), a);
+    pair_mixed_x2_kernel<kThreads, kIptMixed, kTile><<<grid, kThreads, 2 * kTile * sizeof(JBodyX2), cs>>>(
+        reinterpret_cast<const JBodyX2*>(jb), a);
   reduce_splits_kernel<<<(n + 255) / 256, 256, 0, cs>>>(0, n, ld, split, P, SoA6{ax, ay, az, jx, jy, jz});
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)

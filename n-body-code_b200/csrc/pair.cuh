@@ -48,6 +48,53 @@ struct __align__(16) JBody32 {
   float vx, vy, vz, pad1;
 };
 
+// j-record, packed-pair mixed path: every field stored twice so that one
+// 64-bit shared-memory word is a ready (value, value) operand of the f32x2
+// instructions; 96 bytes.
+struct __align__(16) JBodyX2 {
+  float2 xh, yh, zh, m;
+  float2 xl, yl, zl, vx;
+  float2 vy, vz, pad0, pad1;
+};
+
+// Packed single precision (sm_100+): one instruction performs the operation
+// on both halves of a 64-bit register pair.  Same FP32-pipe throughput per
+// lane-op as scalar FMA, half the issue slots.
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ float rcp_mufu(float s) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
+  return y;
+}
+
 __device__ __forceinline__ float rsqrt_mufu(float s) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
@@ -253,6 +300,107 @@ __global__ void __launch_bounds__(NT) pair_mixed_kernel(const JBody32* __restric
         for (int k = 0; k < IPT; ++k) {
           ax[k] += fax[k]; ay[k] += fay[k]; az[k] += faz[k];
           jx[k] += fjx[k]; jy[k] += fjy[k]; jz[k] += fjz[k];
+        }
+      });
+  if (!ok) return;
+
+  double* out = a.out + static_cast<size_t>(split) * 6 * a.stride;
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int i = row0 + k * NT;
+    if (i < a.i_end) {
+      out[0 * a.stride + i] = ax[k];
+      out[1 * a.stride + i] = ay[k];
+      out[2 * a.stride + i] = az[k];
+      out[3 * a.stride + i] = jx[k];
+      out[4 * a.stride + i] = jy[k];
+      out[5 * a.stride + i] = jz[k];
+    }
+  }
+}
+
+// Mixed precision on packed pairs: i-rows (2p, 2p+1) of a thread share one
+// 64-bit register per quantity, so each f32x2 instruction advances two
+// interactions.  Same arithmetic as pair_mixed_kernel except that 1/s comes
+// from the MUFU reciprocal (one FP32-pipe multiply fewer per interaction):
+// y = rsqrt(s), y2 = rcp(s), q = m_j y y2, c = -3 (r.v) y2.
+template <int NT, int IPT, int TJ>
+__global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __restrict__ jb,
+                                                           PairArgs a) {
+  static_assert(IPT % 2 == 0, "rows are processed in pairs");
+  constexpr int NP = IPT / 2;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  JBodyX2* buf = reinterpret_cast<JBodyX2*>(smem_raw);
+  __shared__ uint64_t full[2];
+
+  const int tid = threadIdx.x;
+  const int row0 = a.i_begin + blockIdx.x * (NT * IPT) + tid;
+  const int split = blockIdx.y;
+  const int t_begin = split * a.tiles_per_split;
+  const int nt = max(0, min(a.tiles_per_split, a.n_tiles - t_begin));
+
+  uint64_t xh[NP], yh[NP], zh[NP], xl[NP], yl[NP], zl[NP], ui[NP], vi[NP], wi[NP];
+  uint64_t fax[NP], fay[NP], faz[NP], fjx[NP], fjy[NP], fjz[NP];
+  double ax[IPT], ay[IPT], az[IPT], jx[IPT], jy[IPT], jz[IPT];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const JBodyX2 b0 = jb[min(row0 + (2 * p) * NT, a.n_rows_pad - 1)];
+    const JBodyX2 b1 = jb[min(row0 + (2 * p + 1) * NT, a.n_rows_pad - 1)];
+    xh[p] = f2_pack(b0.xh.x, b1.xh.x); yh[p] = f2_pack(b0.yh.x, b1.yh.x); zh[p] = f2_pack(b0.zh.x, b1.zh.x);
+    xl[p] = f2_pack(b0.xl.x, b1.xl.x); yl[p] = f2_pack(b0.yl.x, b1.yl.x); zl[p] = f2_pack(b0.zl.x, b1.zl.x);
+    ui[p] = f2_pack(b0.vx.x, b1.vx.x); vi[p] = f2_pack(b0.vy.x, b1.vy.x); wi[p] = f2_pack(b0.vz.x, b1.vz.x);
+  }
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    ax[k] = ay[k] = az[k] = 0.0;
+    jx[k] = jy[k] = jz[k] = 0.0;
+  }
+  const float e2f = static_cast<float>(a.eps2);
+  const uint64_t eps2 = f2_pack(e2f, e2f);
+  const uint64_t m3 = f2_pack(-3.0f, -3.0f);
+
+  const bool ok = run_j_tiles<JBodyX2, TJ>(
+      jb, t_begin, nt, buf, full, a.status, [&](const JBodyX2* tile) {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) fax[p] = fay[p] = faz[p] = fjx[p] = fjy[p] = fjz[p] = 0ull;
+#pragma unroll 2
+        for (int j = 0; j < TJ; ++j) {
+          const ulonglong2* r = reinterpret_cast<const ulonglong2*>(tile + j);
+          const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+          // r0 = (xh, yh) r1 = (zh, m) r2 = (xl, yl) r3 = (zl, vx) r4 = (vy, vz)
+#pragma unroll
+          for (int p = 0; p < NP; ++p) {
+            const uint64_t dx = f2_add(f2_sub(r0.x, xh[p]), f2_sub(r2.x, xl[p]));
+            const uint64_t dy = f2_add(f2_sub(r0.y, yh[p]), f2_sub(r2.y, yl[p]));
+            const uint64_t dz = f2_add(f2_sub(r1.x, zh[p]), f2_sub(r3.x, zl[p]));
+            const uint64_t du = f2_sub(r3.y, ui[p]);
+            const uint64_t dv = f2_sub(r4.x, vi[p]);
+            const uint64_t dw = f2_sub(r4.y, wi[p]);
+            const uint64_t s = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, eps2)));
+            const uint64_t rv = f2_fma(dx, du, f2_fma(dy, dv, f2_mul(dz, dw)));
+            float s0, s1;
+            f2_unpack(s, s0, s1);
+            const uint64_t y = f2_pack(rsqrt_mufu(s0), rsqrt_mufu(s1));
+            const uint64_t y2 = f2_pack(rcp_mufu(s0), rcp_mufu(s1));
+            const uint64_t q = f2_mul(r1.y, f2_mul(y, y2));
+            const uint64_t c = f2_mul(rv, f2_mul(y2, m3));
+            fax[p] = f2_fma(q, dx, fax[p]);
+            fay[p] = f2_fma(q, dy, fay[p]);
+            faz[p] = f2_fma(q, dz, faz[p]);
+            fjx[p] = f2_fma(q, f2_fma(c, dx, du), fjx[p]);
+            fjy[p] = f2_fma(q, f2_fma(c, dy, dv), fjy[p]);
+            fjz[p] = f2_fma(q, f2_fma(c, dz, dw), fjz[p]);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          float lo, hi;
+          f2_unpack(fax[p], lo, hi); ax[2 * p] += lo; ax[2 * p + 1] += hi;
+          f2_unpack(fay[p], lo, hi); ay[2 * p] += lo; ay[2 * p + 1] += hi;
+          f2_unpack(faz[p], lo, hi); az[2 * p] += lo; az[2 * p + 1] += hi;
+          f2_unpack(fjx[p], lo, hi); jx[2 * p] += lo; jx[2 * p + 1] += hi;
+          f2_unpack(fjy[p], lo, hi); jy[2 * p] += lo; jy[2 * p + 1] += hi;
+          f2_unpack(fjz[p], lo, hi); jz[2 * p] += lo; jz[2 * p + 1] += hi;
         }
       });
   if (!ok) return;

@@ -45,6 +45,7 @@ class NBodyConfig(C.Structure):
         ("i_per_thread", C.c_int),
         ("j_tile", C.c_int),
         ("split_j", C.c_int),
+        ("pair_variant", C.c_int),
     ]
 
 

@@ -69,6 +69,24 @@ def test_fp64_every_tiling_agrees(tiling):
     assert ea <= TOL_FP64 and ej <= TOL_FP64, (tiling, ea, ej)
 
 
+@pytest.mark.parametrize("tiling", [dict(threads=128, i_per_thread=4, j_tile=128, split_j=1),
+                                    dict(threads=128, i_per_thread=2, j_tile=128, split_j=5),
+                                    dict(threads=256, i_per_thread=2, j_tile=128, split_j=2),
+                                    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64),
+                                    dict(threads=128, i_per_thread=4, j_tile=64, split_j=3),
+                                    dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
+                                    dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1)])
+def test_mixed_every_kernel_agrees(tiling):
+    """Packed-pair and scalar mixed kernels, every shape: same accuracy class."""
+    s = nb.plummer(3000, seed=5)
+    ref = O.force(s, 1e-4)
+    d = engine_derivs(s, 1e-4, precision="mixed", **tiling)
+    ea = vec_rel(d[:3], ref[:3])
+    ej = vec_rel(d[3:], ref[3:])
+    assert np.median(ea) <= 2e-6 and ea.max() <= 2e-4, (tiling, np.median(ea), ea.max())
+    assert np.median(ej) <= 1e-5, (tiling, np.median(ej))
+
+
 def test_dropin_row_range():
     s = nb.plummer(2000, seed=3)
     full = nb.force_calculation(s, eps2=1e-4)
