@@ -65,8 +65,10 @@ typedef struct {
   double eta0;        /* initial-dt criterion, default 1e-4 (nbody.h:15)    */
   int tune;           /* 1: time candidate tilings on first use (autotuner) */
   int threads, i_per_thread, j_tile, split_j; /* 0 = choose automatically   */
-  int pair_variant;   /* mixed only: 0 = packed-pair (f32x2) kernel,
-                         1 = scalar FP32 kernel                             */
+  int pair_variant;   /* mixed only: 0 = packed-pair (f32x2) kernel with
+                         FP64 accumulators in shared memory, 1 = scalar
+                         FP32 kernel, 2 = packed-pair kernel with FP64
+                         accumulators in registers                          */
 } nbody_config;
 
 typedef struct nbody_engine nbody_engine;

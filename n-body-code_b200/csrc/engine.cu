@@ -23,6 +23,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -73,48 +74,66 @@ struct PairKernel {
   int precision, nt, ipt, tj;
   int fmt;      // RecordFormat of the j-records it reads
   const void* fn;
-  size_t smem;  // dynamic shared memory: two j-tile buffers
+  size_t smem;  // dynamic shared memory: two j-tile buffers (+ FP64 accumulators)
+  int acc_smem = 0, junroll = 2;
 };
 
-template <int NT, int IPT, int TJ>
+template <int NT, int IPT, int TJ, int JU = 2>
 PairKernel make_fp64() {
   return {NBODY_FP64, NT, IPT, TJ, kRecF64,
-          reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBody64)};
+          reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ, JU>), 2 * TJ * sizeof(JBody64),
+          0, JU};
 }
 template <int NT, int IPT, int TJ>
 PairKernel make_mixed() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecF32,
           reinterpret_cast<const void*>(&pair_mixed_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBody32)};
 }
-template <int NT, int IPT, int TJ>
+template <int NT, int IPT, int TJ, int ACC = 0, int JU = 2>
 PairKernel make_mixed_x2() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecX2,
-          reinterpret_cast<const void*>(&pair_mixed_x2_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBodyX2)};
+          reinterpret_cast<const void*>(&pair_mixed_x2_kernel<NT, IPT, TJ, ACC, JU>),
+          2 * TJ * sizeof(JBodyX2) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU};
 }
 
-// The first entry of each precision is its default; packed-pair (x2) kernels
-// are preferred over scalar ones of the same shape.
+// The first entry of each shape/variant is the one explicit tilings select;
+// the autotuner times all of them.
 const std::vector<PairKernel>& registry() {
   static const std::vector<PairKernel> r = {
-      make_fp64<128, 2, 128>(),     make_fp64<128, 1, 128>(),     make_fp64<128, 4, 128>(),
-      make_fp64<256, 1, 128>(),     make_fp64<256, 2, 128>(),     make_fp64<128, 2, 256>(),
-      make_fp64<64, 2, 128>(),      make_fp64<64, 4, 128>(),
-      make_mixed_x2<128, 4, 128>(), make_mixed_x2<128, 2, 128>(), make_mixed_x2<256, 2, 128>(),
-      make_mixed_x2<256, 4, 128>(), make_mixed_x2<64, 4, 128>(),  make_mixed_x2<128, 4, 64>(),
+      make_fp64<128, 2, 128, 1>(),  make_fp64<128, 2, 128, 2>(),  make_fp64<128, 1, 128, 4>(),
+      make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
+      make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
+      // packed pairs, FP64 accumulators in shared memory (default)
+      make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
+      make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
+      make_mixed_x2<128, 2, 128, 1, 1>(),
+      // packed pairs, FP64 accumulators in registers
+      make_mixed_x2<128, 4, 128, 0, 2>(), make_mixed_x2<128, 2, 128, 0, 2>(),
+      make_mixed_x2<256, 2, 128, 0, 2>(), make_mixed_x2<64, 4, 128, 0, 2>(),
+      make_mixed_x2<128, 4, 64, 0, 2>(),
+      // scalar FP32
       make_mixed<128, 4, 128>(),    make_mixed<128, 2, 128>(),    make_mixed<256, 2, 128>(),
       make_mixed<128, 4, 256>(),    make_mixed<64, 4, 128>(),
   };
   return r;
 }
 
-// variant (mixed only): 0 = packed-pair kernel when one of that shape
-// exists, 1 = scalar kernel.
+// variant (mixed only): 0 = packed pairs with shared-memory FP64
+// accumulators (falling back to register accumulators where that shape has
+// none), 1 = scalar FP32, 2 = packed pairs with register accumulators.
 const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
-  for (const auto& k : registry())
-    if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj &&
-        (precision == NBODY_FP64 || (variant == 1) == (k.fmt == kRecF32)))
-      return &k;
-  return nullptr;
+  auto match = [&](int fmt, int acc) -> const PairKernel* {
+    for (const auto& k : registry())
+      if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj &&
+          (fmt < 0 || k.fmt == fmt) && (acc < 0 || k.acc_smem == acc))
+        return &k;
+    return nullptr;
+  };
+  if (precision == NBODY_FP64) return match(kRecF64, -1);
+  if (variant == 1) return match(kRecF32, -1);
+  if (variant == 2) return match(kRecX2, 0);
+  const PairKernel* k = match(kRecX2, 1);
+  return k ? k : match(kRecX2, 0);
 }
 
 struct Tiling {
@@ -178,7 +197,10 @@ nbody_status check_status_word(nbody_engine* e) {
 
 // Split count from a wave model: CTAs = i_blocks * S run in waves of
 // (SMs x resident CTAs); each CTA costs its j-tiles plus a fixed overhead.
+nbody_status prepare_kernel(const PairKernel& k);
+
 int choose_split(const nbody_engine* e, const PairKernel& k, int rows) {
+  prepare_kernel(k);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, k.nt, k.smem) != cudaSuccess ||
       occ < 1)
@@ -218,9 +240,26 @@ nbody_status ensure_partials(nbody_engine* e, int split) {
   return NBODY_OK;
 }
 
+// Every pair kernel opts in to its dynamic shared memory size once per
+// device (static + dynamic above 48 KB needs the attribute).
+std::mutex g_prep_mu;
+std::set<std::pair<int, const void*>> g_prepared;
+
+nbody_status prepare_kernel(const PairKernel& k) {
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_prep_mu);
+  if (g_prepared.count({dev, k.fn})) return NBODY_OK;
+  NB_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(k.smem)));
+  g_prepared.insert({dev, k.fn});
+  return NBODY_OK;
+}
+
 nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_end,
                          cudaStream_t st) {
   const PairKernel& k = *t.k;
+  NB_TRY(prepare_kernel(k));
   PairArgs a;
   a.i_begin = i_begin;
   a.i_end = i_end;
@@ -277,8 +316,8 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
       float ms = 0.f;
       NB_CUDA(cudaEventElapsedTime(&ms, a, b));
       if (getenv("NBODY_TUNE_VERBOSE"))
-        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d split=%d  %.4f ms\n",
-                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, s, ms / 3);
+        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d split=%d  %.4f ms\n",
+                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, s, ms / 3);
       if (ms < best) {
         best = ms;
         best_idx = static_cast<int>(idx);
@@ -481,7 +520,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
   if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
-  if (cfg->pair_variant != 0 && cfg->pair_variant != 1)
+  if (cfg->pair_variant < 0 || cfg->pair_variant > 2)
     return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

@@ -165,7 +165,7 @@ struct PairArgs {
   int* status;
 };
 
-template <int NT, int IPT, int TJ>
+template <int NT, int IPT, int TJ, int JU = 2>
 __global__ void __launch_bounds__(NT) pair_fp64_kernel(const JBody64* __restrict__ jb,
                                                        PairArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(NT) pair_fp64_kernel(const JBody64* __restrict
 
   const bool ok = run_j_tiles<JBody64, TJ>(
       jb, t_begin, nt, buf, full, a.status, [&](const JBody64* tile) {
-#pragma unroll 2
+#pragma unroll JU
         for (int j = 0; j < TJ; ++j) {
           const double2* r = reinterpret_cast<const double2*>(tile + j);
           const double2 p0 = r[0], p1 = r[1], p2 = r[2], p3 = r[3];
@@ -324,13 +324,18 @@ __global__ void __launch_bounds__(NT) pair_mixed_kernel(const JBody32* __restric
 // interactions.  Same arithmetic as pair_mixed_kernel except that 1/s comes
 // from the MUFU reciprocal (one FP32-pipe multiply fewer per interaction):
 // y = rsqrt(s), y2 = rcp(s), q = m_j y y2, c = -3 (r.v) y2.
-template <int NT, int IPT, int TJ>
+// ACC_SMEM = 1 keeps the per-row FP64 accumulators in shared memory
+// ([6*IPT][NT] doubles, one column per thread) instead of registers, which
+// frees 12 registers per row for more rows per thread; JU unrolls the j loop.
+template <int NT, int IPT, int TJ, int ACC_SMEM = 0, int JU = 2>
 __global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __restrict__ jb,
                                                            PairArgs a) {
   static_assert(IPT % 2 == 0, "rows are processed in pairs");
   constexpr int NP = IPT / 2;
+  constexpr int NACC = ACC_SMEM ? 1 : IPT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   JBodyX2* buf = reinterpret_cast<JBodyX2*>(smem_raw);
+  double* acc_sm = reinterpret_cast<double*>(smem_raw + 2 * TJ * sizeof(JBodyX2));
   __shared__ uint64_t full[2];
 
   const int tid = threadIdx.x;
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __rest
 
   uint64_t xh[NP], yh[NP], zh[NP], xl[NP], yl[NP], zl[NP], ui[NP], vi[NP], wi[NP];
   uint64_t fax[NP], fay[NP], faz[NP], fjx[NP], fjy[NP], fjz[NP];
-  double ax[IPT], ay[IPT], az[IPT], jx[IPT], jy[IPT], jz[IPT];
+  double ax[NACC], ay[NACC], az[NACC], jx[NACC], jy[NACC], jz[NACC];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     const JBodyX2 b0 = jb[min(row0 + (2 * p) * NT, a.n_rows_pad - 1)];
@@ -351,19 +356,37 @@ __global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __rest
     ui[p] = f2_pack(b0.vx.x, b1.vx.x); vi[p] = f2_pack(b0.vy.x, b1.vy.x); wi[p] = f2_pack(b0.vz.x, b1.vz.x);
   }
 #pragma unroll
-  for (int k = 0; k < IPT; ++k) {
+  for (int k = 0; k < NACC; ++k) {
     ax[k] = ay[k] = az[k] = 0.0;
     jx[k] = jy[k] = jz[k] = 0.0;
+  }
+  if (ACC_SMEM) {
+#pragma unroll
+    for (int r = 0; r < 6 * IPT; ++r) acc_sm[r * NT + tid] = 0.0;
   }
   const float e2f = static_cast<float>(a.eps2);
   const uint64_t eps2 = f2_pack(e2f, e2f);
   const uint64_t m3 = f2_pack(-3.0f, -3.0f);
 
+  // adds the float pair (lo, hi) of field c, pair p into the FP64 accumulators
+  auto flush = [&](int c, int p, uint64_t v) {
+    float lo, hi;
+    f2_unpack(v, lo, hi);
+    if (ACC_SMEM) {
+      acc_sm[(c * IPT + 2 * p) * NT + tid] += lo;
+      acc_sm[(c * IPT + 2 * p + 1) * NT + tid] += hi;
+    } else {
+      double* f = c == 0 ? ax : c == 1 ? ay : c == 2 ? az : c == 3 ? jx : c == 4 ? jy : jz;
+      f[(2 * p) % NACC] += lo;
+      f[(2 * p + 1) % NACC] += hi;
+    }
+  };
+
   const bool ok = run_j_tiles<JBodyX2, TJ>(
       jb, t_begin, nt, buf, full, a.status, [&](const JBodyX2* tile) {
 #pragma unroll
         for (int p = 0; p < NP; ++p) fax[p] = fay[p] = faz[p] = fjx[p] = fjy[p] = fjz[p] = 0ull;
-#pragma unroll 2
+#pragma unroll JU
         for (int j = 0; j < TJ; ++j) {
           const ulonglong2* r = reinterpret_cast<const ulonglong2*>(tile + j);
           const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
@@ -394,13 +417,8 @@ __global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __rest
         }
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
-          float lo, hi;
-          f2_unpack(fax[p], lo, hi); ax[2 * p] += lo; ax[2 * p + 1] += hi;
-          f2_unpack(fay[p], lo, hi); ay[2 * p] += lo; ay[2 * p + 1] += hi;
-          f2_unpack(faz[p], lo, hi); az[2 * p] += lo; az[2 * p + 1] += hi;
-          f2_unpack(fjx[p], lo, hi); jx[2 * p] += lo; jx[2 * p + 1] += hi;
-          f2_unpack(fjy[p], lo, hi); jy[2 * p] += lo; jy[2 * p + 1] += hi;
-          f2_unpack(fjz[p], lo, hi); jz[2 * p] += lo; jz[2 * p + 1] += hi;
+          flush(0, p, fax[p]); flush(1, p, fay[p]); flush(2, p, faz[p]);
+          flush(3, p, fjx[p]); flush(4, p, fjy[p]); flush(5, p, fjz[p]);
         }
       });
   if (!ok) return;
@@ -410,12 +428,17 @@ __global__ void __launch_bounds__(NT) pair_mixed_x2_kernel(const JBodyX2* __rest
   for (int k = 0; k < IPT; ++k) {
     const int i = row0 + k * NT;
     if (i < a.i_end) {
-      out[0 * a.stride + i] = ax[k];
-      out[1 * a.stride + i] = ay[k];
-      out[2 * a.stride + i] = az[k];
-      out[3 * a.stride + i] = jx[k];
-      out[4 * a.stride + i] = jy[k];
-      out[5 * a.stride + i] = jz[k];
+      if (ACC_SMEM) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) out[c * a.stride + i] = acc_sm[(c * IPT + k) * NT + tid];
+      } else {
+        out[0 * a.stride + i] = ax[k % NACC];
+        out[1 * a.stride + i] = ay[k % NACC];
+        out[2 * a.stride + i] = az[k % NACC];
+        out[3 * a.stride + i] = jx[k % NACC];
+        out[4 * a.stride + i] = jy[k % NACC];
+        out[5 * a.stride + i] = jz[k % NACC];
+      }
     }
   }
 }

@@ -75,7 +75,10 @@ def test_fp64_every_tiling_agrees(tiling):
                                     dict(threads=64, i_per_thread=4, j_tile=128, split_j=64),
                                     dict(threads=128, i_per_thread=4, j_tile=64, split_j=3),
                                     dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
-                                    dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1)])
+                                    dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1),
+                                    dict(threads=128, i_per_thread=4, j_tile=128, split_j=9, pair_variant=2),
+                                    dict(threads=256, i_per_thread=4, j_tile=128, split_j=4),
+                                    dict(threads=128, i_per_thread=2, j_tile=128, split_j=11)])
 def test_mixed_every_kernel_agrees(tiling):
     """Packed-pair and scalar mixed kernels, every shape: same accuracy class."""
     s = nb.plummer(3000, seed=5)
