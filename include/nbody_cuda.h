@@ -127,6 +127,8 @@ nbody_status nbody_synchronize(nbody_engine* eng);
 nbody_status nbody_energy(nbody_engine* eng, int ref_compat, double* T, double* U);
 
 nbody_status nbody_get_timers(nbody_engine* eng, nbody_timers* out);
+/* Set model time and (if dt > 0) the current shared step, e.g. on resume. */
+nbody_status nbody_set_time(nbody_engine* eng, double t, double dt);
 /* The engine's CUDA stream (cudaStream_t), for callers that order their own
  * work against it. */
 nbody_status nbody_get_stream(nbody_engine* eng, void** stream);
@@ -192,6 +194,18 @@ nbody_status nbody_plummer(int n, uint64_t seed, double* x, double* y, double* z
  * reference potential at eps2) - the config-1 bodies. */
 nbody_status nbody_reference_ic(int n, double eps2, double* x, double* y, double* z, double* m,
                                 double* vx, double* vy, double* vz);
+
+/* ---- state files (host) -----------------------------------------------------
+ * Binary SoA snapshot: 64-byte header ("NBODYST1", version 1, n, t, dt, eps2)
+ * then x, y, z, m, vx, vy, vz as float64.  Reading with all array pointers
+ * NULL returns the header only (n, t, dt, eps2). */
+nbody_status nbody_write_state_file(const char* path, int n, double t, double dt, double eps2,
+                                    const double* x, const double* y, const double* z,
+                                    const double* m, const double* vx, const double* vy,
+                                    const double* vz);
+nbody_status nbody_read_state_file(const char* path, int n_max, int* n, double* t, double* dt,
+                                   double* eps2, double* x, double* y, double* z, double* m,
+                                   double* vx, double* vy, double* vz);
 
 /* ---- measured pipe peaks (diagnostic) ---------------------------------------
  * Times FP64 FMA, FP32 FMA and MUFU rsqrt throughput on `device` with

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-ccbin", "/usr/bin/g++"]
 
-LIB_SOURCES = ["engine.cu", "peaks.cu", "noalloc.cu", "ensemble.cu", "adjoint.cu", "ic.cpp"]
+LIB_SOURCES = ["engine.cu", "peaks.cu", "noalloc.cu", "ensemble.cu", "adjoint.cu", "ic.cpp", "state_io.cpp"]
 
 
 def _sources(names, base):

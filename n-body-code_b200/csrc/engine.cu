@@ -733,6 +733,18 @@ nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
   return NBODY_OK;
 }
 
+nbody_status nbody_set_time(nbody_engine* e, double t, double dt) {
+  NB_TRY(need_state(e));
+  if (!std::isfinite(t)) return fail(NBODY_ERR_INVALID_ARG, "t is not finite");
+  StepCtl c;
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  NB_CUDA(cudaMemcpy(&c, e->ctl, sizeof c, cudaMemcpyDeviceToHost));
+  c.t = t;
+  if (dt > 0) c.dt = dt;
+  NB_CUDA(cudaMemcpy(e->ctl, &c, sizeof c, cudaMemcpyHostToDevice));
+  return NBODY_OK;
+}
+
 nbody_status nbody_get_stream(nbody_engine* e, void** stream) {
   NB_TRY(check_engine(e));
   if (!stream) return fail(NBODY_ERR_INVALID_ARG, "null stream out");

@@ -61,7 +61,8 @@ def test_fp64_force_vs_oracle_plummer(n):
 @pytest.mark.parametrize("tiling", [dict(threads=128, i_per_thread=1, j_tile=128, split_j=1),
                                     dict(threads=128, i_per_thread=4, j_tile=128, split_j=7),
                                     dict(threads=256, i_per_thread=2, j_tile=128, split_j=3),
-                                    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64)])
+                                    dict(threads=64, i_per_thread=2, j_tile=128, split_j=64),
+                                    dict(threads=128, i_per_thread=2, j_tile=256, split_j=5)])
 def test_fp64_every_tiling_agrees(tiling):
     s = nb.plummer(3000, seed=5)
     d = engine_derivs(s, 1e-4, **tiling)
