@@ -183,6 +183,50 @@ nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision, const dou
                                     double* ax, double* ay, double* az, double* jx, double* jy,
                                     double* jz, void* stream);
 
+/* ---- batched ensembles -------------------------------------------------------
+ * Many independent systems ("clusters") of uneven size, advanced together:
+ * each Hermite step is one persistent pair launch over a work list of
+ * (cluster, 256-row block, j-tile range) items, captured with the O(N)
+ * kernels in one CUDA graph.  No reference counterpart (the reference runs one
+ * system); per cluster the physics is exactly the single-system engine's.
+ * Each cluster has its own softening and fixed shared step.  State arrays are
+ * the clusters' bodies concatenated in cluster order (sum n[c] values each). */
+typedef struct nbody_ensemble nbody_ensemble;
+typedef struct {
+  int nclusters;
+  const int* n;          /* bodies per cluster (>= 1)                        */
+  const double* eps2;    /* softening^2 per cluster                          */
+  const double* dt;      /* fixed shared step per cluster (> 0)              */
+  int precision;         /* nbody_precision                                  */
+  int device;
+  int tiles_per_item;    /* j-tiles (128 bodies) per work item; 0 = default 8,
+                            or chosen by timing when tune = 1               */
+  int tune;
+} nbody_ensemble_config;
+typedef struct {
+  int nclusters, padded_rows, items, tiles_per_item, grid;
+  double interactions_per_step;  /* sum of n[c]^2 */
+  long long steps;
+  double last_step_ms;           /* CUDA events around the last graph step */
+} nbody_ensemble_info_t;
+
+nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_config* cfg);
+nbody_status nbody_ensemble_destroy(nbody_ensemble* ens);
+nbody_status nbody_ensemble_set_state(nbody_ensemble* ens, const double* x, const double* y,
+                                      const double* z, const double* m, const double* vx,
+                                      const double* vy, const double* vz);
+nbody_status nbody_ensemble_get_state(nbody_ensemble* ens, double* x, double* y, double* z,
+                                      double* vx, double* vy, double* vz);
+nbody_status nbody_ensemble_get_derivs(nbody_ensemble* ens, double* ax, double* ay, double* az,
+                                       double* jx, double* jy, double* jz);
+nbody_status nbody_ensemble_acc_jerk(nbody_ensemble* ens);
+nbody_status nbody_ensemble_step(nbody_ensemble* ens, int nsteps);
+nbody_status nbody_ensemble_synchronize(nbody_ensemble* ens);
+/* Per-cluster FP64 kinetic and potential energy (arrays of nclusters). */
+nbody_status nbody_ensemble_energy(nbody_ensemble* ens, double* T, double* U);
+nbody_status nbody_ensemble_info(nbody_ensemble* ens, nbody_ensemble_info_t* out);
+nbody_status nbody_ensemble_get_stream(nbody_ensemble* ens, void** stream);
+
 /* ---- initial conditions (host, deterministic) ------------------------------
  * Plummer sphere in Henon units (G = M = 1, E = -1/4), equal masses 1/n,
  * centred on the origin in position and velocity; sampled by the

@@ -1,0 +1,641 @@
+// Batched ensembles: many independent systems ("clusters") of uneven size
+// advanced together, one persistent pair launch per Hermite step.
+//
+// Layout: cluster c owns padded rows [row0_c, row0_c + ld_c) of every
+// ensemble array (ld_c = n_c rounded up to 256), so j-tiles never straddle
+// clusters and padding rows are zero-mass bodies that add nothing.  A row's
+// cluster comes from cid[row] (-1 on padding rows).
+//
+// Work list: item = (cluster, 256-row block, j-tile range of at most
+// `tiles_per_item` tiles).  Items are sorted by cost (longest first) and a
+// fixed grid of SMs x resident CTAs takes them from an atomic counter, so a
+// 256-body cluster and an 8192-body cluster share one launch without the
+// small one idling the GPU.  Split partial sums of cluster c live at
+// P + p_off_c ([S_c][6][ld_c]) and are added in a fixed order by the
+// corrector, so results are bitwise reproducible.
+//
+// A step is memset(counter) -> predict -> persistent pair -> correct,
+// captured once into a CUDA graph.  Each cluster has its own softening and
+// fixed shared step (the adaptive criterion is per system in the reference,
+// src/nbody.cpp:198-222; ensembles here run fixed steps).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "../../include/nbody_cuda.h"
+#include "errors.h"
+#include "hermite.cuh"
+#include "pair.cuh"
+
+using namespace nbody;
+
+namespace {
+
+constexpr int kPadRows = 256;  // cluster padding = rows per work item
+constexpr int kTile = 128;     // j-tile size of the ensemble kernels
+constexpr int kBlock = 256;
+
+using RowsEnsFP64 = RowsFP64<128, 2, kTile, 1>;              // 256 rows
+using RowsEnsMixed = RowsMixedX2<64, 4, kTile, 1, 1>;        // 256 rows
+static_assert(RowsEnsFP64::ROWS == kPadRows && RowsEnsMixed::ROWS == kPadRows,
+              "an item's row block is one padding unit");
+
+struct ClusterDev {
+  int row0, n, ld, S;
+  long long p_off;
+  double eps2, dt;
+};
+
+#define EN_CUDA(call)                                                                      \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return nbody_set_error(e_ == cudaErrorMemoryAllocation ? NBODY_ERR_OOM : NBODY_ERR_CUDA, \
+                             "%s failed: %s", #call, cudaGetErrorString(e_));              \
+  } while (0)
+#define EN_TRY(expr)               \
+  do {                             \
+    nbody_status s_ = (expr);      \
+    if (s_ != NBODY_OK) return s_; \
+  } while (0)
+
+// ---- kernels ----------------------------------------------------------------
+
+__global__ void ens_pack_kernel(int L, const int* __restrict__ cid, const double* __restrict__ X,
+                                const double* __restrict__ V, const double* __restrict__ M,
+                                JBody64* __restrict__ jb64, JBodyX2* __restrict__ jbx) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L) return;
+  const bool real = cid[r] >= 0;
+  const double x = real ? X[r] : 0, y = real ? X[L + r] : 0, z = real ? X[2 * L + r] : 0;
+  const double m = real ? M[r] : 0;
+  const double u = real ? V[r] : 0, v = real ? V[L + r] : 0, w = real ? V[2 * L + r] : 0;
+  if (jb64) {
+    JBody64 b;
+    b.x = x; b.y = y; b.z = z; b.m = m; b.vx = u; b.vy = v; b.vz = w; b.pad = 0;
+    jb64[r] = b;
+  }
+  if (jbx) jbx[r] = make_jbx2(x, y, z, m, u, v, w);
+}
+
+__global__ void ens_predict_kernel(int L, const int* __restrict__ cid,
+                                   const ClusterDev* __restrict__ cl, double* __restrict__ X,
+                                   double* __restrict__ V, const double* __restrict__ M,
+                                   const double* __restrict__ D, JBody64* __restrict__ jb64,
+                                   JBodyX2* __restrict__ jbx) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L) return;
+  const int c = cid[r];
+  if (c < 0) return;
+  const double dt = cl[c].dt;
+  const double h2 = 0.5 * dt * dt;
+  const double h3 = dt * dt * dt * (1.0 / 6.0);
+  double p[3], u[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double x = X[k * L + r], v = V[k * L + r];
+    const double a = D[k * L + r], j = D[(3 + k) * L + r];
+    p[k] = x + (v * dt + (a * h2 + j * h3));
+    u[k] = v + (a * dt + j * h2);
+    X[k * L + r] = p[k];
+    V[k * L + r] = u[k];
+  }
+  const double m = M[r];
+  if (jb64) {
+    JBody64 b;
+    b.x = p[0]; b.y = p[1]; b.z = p[2]; b.m = m; b.vx = u[0]; b.vy = u[1]; b.vz = u[2]; b.pad = 0;
+    jb64[r] = b;
+  }
+  if (jbx) jbx[r] = make_jbx2(p[0], p[1], p[2], m, u[0], u[1], u[2]);
+}
+
+// Sum of a row's split partials, field f.
+__device__ __forceinline__ double ens_split_sum(const double* __restrict__ P, const ClusterDev& k,
+                                                int f, int i) {
+  double v = 0.0;
+  for (int s = 0; s < k.S; ++s) v += P[k.p_off + (static_cast<long long>(s) * 6 + f) * k.ld + i];
+  return v;
+}
+
+__global__ void ens_correct_kernel(int L, const int* __restrict__ cid,
+                                   const ClusterDev* __restrict__ cl, const double* __restrict__ P,
+                                   double* __restrict__ X, double* __restrict__ V,
+                                   double* __restrict__ D) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L) return;
+  const int c = cid[r];
+  if (c < 0) return;
+  const ClusterDev k = cl[c];
+  const int i = r - k.row0;
+  const double dt = k.dt;
+  const double idt2 = 1.0 / (dt * dt), idt3 = idt2 / dt;
+  const double dt3 = dt * dt * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double a1 = ens_split_sum(P, k, q, i), j1 = ens_split_sum(P, k, 3 + q, i);
+    const double a = D[q * L + r], j = D[(3 + q) * L + r];
+    const double da = a - a1;
+    const double a2 = 2.0 * idt2 * (-3.0 * da - (2.0 * j + j1) * dt);
+    const double a3 = 6.0 * idt3 * (2.0 * da + (j + j1) * dt);
+    X[q * L + r] += a2 * dt4 * (1.0 / 24.0) + a3 * dt5 * (1.0 / 120.0);
+    V[q * L + r] += a2 * dt3 * (1.0 / 6.0) + a3 * dt4 * (1.0 / 24.0);
+    D[q * L + r] = a1;
+    D[(3 + q) * L + r] = j1;
+  }
+}
+
+__global__ void ens_reduce_kernel(int L, const int* __restrict__ cid,
+                                  const ClusterDev* __restrict__ cl, const double* __restrict__ P,
+                                  double* __restrict__ D) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L) return;
+  const int c = cid[r];
+  if (c < 0) return;
+  const ClusterDev k = cl[c];
+  for (int f = 0; f < 6; ++f) D[f * L + r] = ens_split_sum(P, k, f, r - k.row0);
+}
+
+// phi[r] = sum over the same cluster's j != r of m_j / sqrt(r^2 + eps2_c);
+// one CTA per 256-row block, blocks listed in `blk` as cluster ids.
+__global__ void __launch_bounds__(kBlock) ens_phi_kernel(const int* __restrict__ blk_cluster,
+                                                         const int* __restrict__ blk_row,
+                                                         const ClusterDev* __restrict__ cl,
+                                                         const JBody64* __restrict__ jb,
+                                                         double* __restrict__ phi) {
+  __shared__ double4 tile[kBlock];
+  const ClusterDev k = cl[blk_cluster[blockIdx.x]];
+  const int i = blk_row[blockIdx.x] + threadIdx.x;  // cluster-relative row
+  const JBody64 bi = jb[k.row0 + i];
+  double acc = 0.0;
+  for (int j0 = 0; j0 < k.ld; j0 += kBlock) {
+    const JBody64 bj = jb[k.row0 + j0 + threadIdx.x];
+    tile[threadIdx.x] = make_double4(bj.x, bj.y, bj.z, bj.m);
+    __syncthreads();
+#pragma unroll 4
+    for (int t = 0; t < kBlock; ++t) {
+      const double4 p = tile[t];
+      const double dx = p.x - bi.x, dy = p.y - bi.y, dz = p.z - bi.z;
+      const double y = rsqrt_f64(fma(dx, dx, fma(dy, dy, fma(dz, dz, k.eps2))));
+      acc += (j0 + t != i) ? p.w * y : 0.0;
+    }
+    __syncthreads();
+  }
+  phi[k.row0 + i] = acc;
+}
+
+// Per cluster (one CTA each): T = sum 0.5 m v^2, U = -0.5 sum m phi.
+__global__ void ens_energy_sum_kernel(const ClusterDev* __restrict__ cl, const double* __restrict__ V,
+                                      const double* __restrict__ M, const double* __restrict__ phi,
+                                      int L, double* __restrict__ T, double* __restrict__ U) {
+  __shared__ double sh[32];
+  const ClusterDev k = cl[blockIdx.x];
+  double t = 0.0, u = 0.0;
+  for (int i = threadIdx.x; i < k.n; i += blockDim.x) {
+    const int r = k.row0 + i;
+    const double a = V[r], b = V[L + r], c = V[2 * L + r];
+    t += 0.5 * M[r] * (a * a + b * b + c * c);
+    u += M[r] * phi[r];
+  }
+  const double bt = block_sum(t, sh);
+  const double bu = block_sum(u, sh);
+  if (threadIdx.x == 0) {
+    T[blockIdx.x] = bt;
+    U[blockIdx.x] = -0.5 * bu;
+  }
+}
+
+template <class R>
+const void* ens_kernel() {
+  return reinterpret_cast<const void*>(&ensemble_pair_kernel<R>);
+}
+
+}  // namespace
+
+struct nbody_ensemble {
+  int C = 0, L = 0, dev = 0, sms = 0, precision = 0;
+  int tiles_per_item = 8;
+  int grid = 0;
+  long long interactions = 0;  // sum of n_c^2 per step
+  cudaStream_t stream = nullptr;
+  std::vector<int> n, row0, ld;
+  std::vector<double> eps2, dt;
+  double* state = nullptr;  // [13][L]
+  double *X = nullptr, *V = nullptr, *M = nullptr, *D = nullptr;
+  double* P = nullptr;
+  size_t p_doubles = 0;
+  JBody64* jb64 = nullptr;
+  JBodyX2* jbx = nullptr;
+  int* cid = nullptr;
+  ClusterDev* cl = nullptr;
+  EnsItem* items = nullptr;
+  int n_items = 0;
+  unsigned int* counter = nullptr;
+  int* status = nullptr;
+  int *blk_cluster = nullptr, *blk_row = nullptr;
+  int n_blk = 0;
+  double *phi = nullptr, *Tc = nullptr, *Uc = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool have_derivs = false;
+  long long steps = 0;
+};
+
+namespace {
+
+nbody_status ens_status(nbody_ensemble* e) {
+  int h = 0;
+  EN_CUDA(cudaMemcpyAsync(&h, e->status, sizeof h, cudaMemcpyDeviceToHost, e->stream));
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  if (h) {
+    cudaMemsetAsync(e->status, 0, sizeof(int), e->stream);
+    return nbody_set_error(NBODY_ERR_TIMEOUT, "an ensemble pair-kernel wait exceeded its limit");
+  }
+  return NBODY_OK;
+}
+
+// (Re)builds the work list and partial-sum layout for `tpi` tiles per item.
+nbody_status build_items(nbody_ensemble* e, int tpi) {
+  std::vector<ClusterDev> cl(e->C);
+  std::vector<EnsItem> items;
+  long long p_off = 0;
+  for (int c = 0; c < e->C; ++c) {
+    const int tiles = e->ld[c] / kTile;
+    const int S = (tiles + tpi - 1) / tpi;
+    cl[c] = ClusterDev{e->row0[c], e->n[c], e->ld[c], S, p_off, e->eps2[c], e->dt[c]};
+    for (int rb = 0; rb < e->ld[c] / kPadRows; ++rb)
+      for (int s = 0; s < S; ++s) {
+        EnsItem it;
+        it.jrow0 = e->row0[c];
+        it.row0 = rb * kPadRows;
+        it.rows_end = e->n[c];
+        it.ld = e->ld[c];
+        it.t_begin = s * tpi;
+        it.nt = std::min(tpi, tiles - it.t_begin);
+        it.out_off = p_off + static_cast<long long>(s) * 6 * e->ld[c];
+        it.eps2 = e->eps2[c];
+        items.push_back(it);
+      }
+    p_off += static_cast<long long>(S) * 6 * e->ld[c];
+  }
+  // longest items first, then by cluster so neighbours share L2 lines
+  std::stable_sort(items.begin(), items.end(),
+                   [](const EnsItem& a, const EnsItem& b) { return a.nt > b.nt; });
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  cudaFree(e->P);
+  cudaFree(e->items);
+  e->P = nullptr;
+  e->items = nullptr;
+  e->p_doubles = static_cast<size_t>(p_off);
+  EN_CUDA(cudaMalloc(&e->P, sizeof(double) * e->p_doubles));
+  EN_CUDA(cudaMalloc(&e->items, sizeof(EnsItem) * items.size()));
+  EN_CUDA(cudaMemcpy(e->items, items.data(), sizeof(EnsItem) * items.size(), cudaMemcpyHostToDevice));
+  EN_CUDA(cudaMemcpy(e->cl, cl.data(), sizeof(ClusterDev) * e->C, cudaMemcpyHostToDevice));
+  e->n_items = static_cast<int>(items.size());
+  e->tiles_per_item = tpi;
+  return NBODY_OK;
+}
+
+nbody_status launch_ens_pair(nbody_ensemble* e) {
+  EN_CUDA(cudaMemsetAsync(e->counter, 0, sizeof(unsigned int), e->stream));
+  const bool fp64 = e->precision == NBODY_FP64;
+  const void* fn = fp64 ? ens_kernel<RowsEnsFP64>() : ens_kernel<RowsEnsMixed>();
+  const size_t smem = fp64 ? pair_smem_bytes<RowsEnsFP64>() : pair_smem_bytes<RowsEnsMixed>();
+  const int nt = fp64 ? RowsEnsFP64::NT : RowsEnsMixed::NT;
+  const void* jb = fp64 ? static_cast<const void*>(e->jb64) : static_cast<const void*>(e->jbx);
+  void* args[] = {const_cast<void*>(static_cast<const void*>(&jb)), &e->items, &e->n_items,
+                  &e->counter, &e->P, &e->status};
+  EN_CUDA(cudaLaunchKernel(fn, dim3(e->grid), dim3(nt), args, smem, e->stream));
+  return NBODY_OK;
+}
+
+nbody_status launch_ens_pack(nbody_ensemble* e) {
+  const bool fp64 = e->precision == NBODY_FP64;
+  ens_pack_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
+      e->L, e->cid, e->X, e->V, e->M, e->jb64, fp64 ? nullptr : e->jbx);
+  EN_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+nbody_status ens_eval_current(nbody_ensemble* e) {
+  EN_TRY(launch_ens_pack(e));
+  EN_TRY(launch_ens_pair(e));
+  ens_reduce_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->cid, e->cl,
+                                                                          e->P, e->D);
+  EN_CUDA(cudaGetLastError());
+  e->have_derivs = true;
+  return NBODY_OK;
+}
+
+nbody_status ens_build_graph(nbody_ensemble* e) {
+  if (e->graph) return NBODY_OK;
+  const bool fp64 = e->precision == NBODY_FP64;
+  cudaGraph_t g = nullptr;
+  EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  nbody_status s = NBODY_OK;
+  if (cudaEventRecordWithFlags(e->ev[0], e->stream, cudaEventRecordExternal) != cudaSuccess)
+    s = nbody_set_error(NBODY_ERR_CUDA, "event record during capture failed");
+  ens_predict_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
+      e->L, e->cid, e->cl, e->X, e->V, e->M, e->D, fp64 ? e->jb64 : nullptr,
+      fp64 ? nullptr : e->jbx);
+  if (s == NBODY_OK) s = launch_ens_pair(e);
+  ens_correct_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->cid, e->cl,
+                                                                           e->P, e->X, e->V, e->D);
+  if (s == NBODY_OK && cudaEventRecordWithFlags(e->ev[1], e->stream, cudaEventRecordExternal) != cudaSuccess)
+    s = nbody_set_error(NBODY_ERR_CUDA, "event record during capture failed");
+  cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+  if (s != NBODY_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (ce != cudaSuccess) return nbody_set_error(NBODY_ERR_CUDA, "capture: %s", cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    e->graph = nullptr;
+    return nbody_set_error(NBODY_ERR_CUDA, "instantiate: %s", cudaGetErrorString(ce));
+  }
+  return NBODY_OK;
+}
+
+// Times the pair launch for each candidate item size; keeps the fastest.
+nbody_status ens_autotune(nbody_ensemble* e) {
+  EN_TRY(launch_ens_pack(e));
+  cudaEvent_t a, b;
+  EN_CUDA(cudaEventCreate(&a));
+  EN_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_tpi = e->tiles_per_item;
+  for (int tpi : {2, 4, 8, 16, 32, 64}) {
+    EN_TRY(build_items(e, tpi));
+    EN_TRY(launch_ens_pair(e));
+    EN_CUDA(cudaEventRecord(a, e->stream));
+    for (int r = 0; r < 2; ++r) EN_TRY(launch_ens_pair(e));
+    EN_CUDA(cudaEventRecord(b, e->stream));
+    EN_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    EN_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (ms < best) {
+      best = ms;
+      best_tpi = tpi;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  EN_TRY(ens_status(e));
+  return build_items(e, best_tpi);
+}
+
+nbody_status ens_check(nbody_ensemble* e) {
+  if (!e) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null ensemble");
+  if (cudaSetDevice(e->dev) != cudaSuccess) return nbody_set_error(NBODY_ERR_CUDA, "cudaSetDevice failed");
+  return NBODY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nbody_status nbody_ensemble_destroy(nbody_ensemble* e) {
+  if (!e) return NBODY_OK;
+  cudaSetDevice(e->dev);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (auto ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
+  void* bufs[] = {e->state, e->P, e->jb64, e->jbx, e->cid, e->cl, e->items, e->counter,
+                  e->status, e->blk_cluster, e->blk_row, e->phi, e->Tc, e->Uc};
+  for (void* p : bufs) cudaFree(p);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_config* cfg) {
+  if (!out || !cfg || !cfg->n || !cfg->eps2 || !cfg->dt)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG, "null ensemble argument");
+  *out = nullptr;
+  const int C = cfg->nclusters;
+  if (C < 1) return nbody_set_error(NBODY_ERR_INVALID_ARG, "nclusters = %d", C);
+  if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
+  if (cfg->tiles_per_item < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "tiles_per_item < 0");
+  long long L = 0;
+  for (int c = 0; c < C; ++c) {
+    if (cfg->n[c] < 1) return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d has n = %d", c, cfg->n[c]);
+    if (!(cfg->eps2[c] >= 1e-30 && cfg->eps2[c] <= 1e30))
+      return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d eps2 = %g", c, cfg->eps2[c]);
+    if (!(cfg->dt[c] > 0)) return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d dt = %g (ensembles use fixed steps)", c, cfg->dt[c]);
+    L += (cfg->n[c] + kPadRows - 1) / kPadRows * kPadRows;
+  }
+  if (L > (1LL << 28)) return nbody_set_error(NBODY_ERR_INVALID_ARG, "ensemble too large");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return nbody_set_error(NBODY_ERR_NO_DEVICE, "no CUDA device visible");
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG, "device %d of %d", cfg->device, ndev);
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cfg->device);
+  if (major != 10) return nbody_set_error(NBODY_ERR_NO_DEVICE, "device %d is not sm_100", cfg->device);
+  EN_CUDA(cudaSetDevice(cfg->device));
+
+  std::unique_ptr<nbody_ensemble> e(new nbody_ensemble);
+  e->C = C;
+  e->L = static_cast<int>(L);
+  e->dev = cfg->device;
+  e->precision = cfg->precision;
+  cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->dev);
+  e->n.assign(cfg->n, cfg->n + C);
+  e->eps2.assign(cfg->eps2, cfg->eps2 + C);
+  e->dt.assign(cfg->dt, cfg->dt + C);
+  std::vector<int> cid(e->L, -1), blk_cluster, blk_row;
+  int r0 = 0;
+  for (int c = 0; c < C; ++c) {
+    const int ld = (e->n[c] + kPadRows - 1) / kPadRows * kPadRows;
+    e->row0.push_back(r0);
+    e->ld.push_back(ld);
+    for (int i = 0; i < e->n[c]; ++i) cid[r0 + i] = c;
+    for (int b = 0; b < ld; b += kPadRows) {
+      blk_cluster.push_back(c);
+      blk_row.push_back(b);
+    }
+    e->interactions += static_cast<long long>(e->n[c]) * e->n[c];
+    r0 += ld;
+  }
+  e->n_blk = static_cast<int>(blk_cluster.size());
+  nbody_ensemble* raw = e.get();
+  auto body = [&]() -> nbody_status {
+    EN_CUDA(cudaStreamCreateWithFlags(&raw->stream, cudaStreamNonBlocking));
+    const size_t Ls = raw->L;
+    EN_CUDA(cudaMalloc(&raw->state, sizeof(double) * 13 * Ls));
+    EN_CUDA(cudaMemset(raw->state, 0, sizeof(double) * 13 * Ls));
+    raw->X = raw->state;
+    raw->V = raw->state + 3 * Ls;
+    raw->M = raw->state + 6 * Ls;
+    raw->D = raw->state + 7 * Ls;
+    EN_CUDA(cudaMalloc(&raw->jb64, sizeof(JBody64) * Ls));
+    if (raw->precision == NBODY_MIXED) EN_CUDA(cudaMalloc(&raw->jbx, sizeof(JBodyX2) * Ls));
+    EN_CUDA(cudaMalloc(&raw->cid, sizeof(int) * Ls));
+    EN_CUDA(cudaMemcpy(raw->cid, cid.data(), sizeof(int) * Ls, cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMalloc(&raw->cl, sizeof(ClusterDev) * raw->C));
+    EN_CUDA(cudaMalloc(&raw->counter, sizeof(unsigned int)));
+    EN_CUDA(cudaMalloc(&raw->status, sizeof(int)));
+    EN_CUDA(cudaMemset(raw->status, 0, sizeof(int)));
+    EN_CUDA(cudaMalloc(&raw->blk_cluster, sizeof(int) * raw->n_blk));
+    EN_CUDA(cudaMalloc(&raw->blk_row, sizeof(int) * raw->n_blk));
+    EN_CUDA(cudaMemcpy(raw->blk_cluster, blk_cluster.data(), sizeof(int) * raw->n_blk, cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMemcpy(raw->blk_row, blk_row.data(), sizeof(int) * raw->n_blk, cudaMemcpyHostToDevice));
+    EN_CUDA(cudaMalloc(&raw->phi, sizeof(double) * Ls));
+    EN_CUDA(cudaMalloc(&raw->Tc, sizeof(double) * raw->C));
+    EN_CUDA(cudaMalloc(&raw->Uc, sizeof(double) * raw->C));
+    for (auto& ev : raw->ev) EN_CUDA(cudaEventCreate(&ev));
+    const bool fp64 = raw->precision == NBODY_FP64;
+    const void* fn = fp64 ? ens_kernel<RowsEnsFP64>() : ens_kernel<RowsEnsMixed>();
+    const size_t smem = fp64 ? pair_smem_bytes<RowsEnsFP64>() : pair_smem_bytes<RowsEnsMixed>();
+    const int nt = fp64 ? RowsEnsFP64::NT : RowsEnsMixed::NT;
+    EN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int occ = 0;
+    EN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nt, smem));
+    raw->grid = raw->sms * std::max(occ, 1);
+    return build_items(raw, cfg->tiles_per_item > 0 ? cfg->tiles_per_item : 8);
+  };
+  nbody_status s = body();
+  if (s != NBODY_OK) {
+    nbody_ensemble_destroy(e.release());
+    return s;
+  }
+  if (cfg->tune && cfg->tiles_per_item == 0) e->tiles_per_item = -1;  // tune at first state
+  *out = e.release();
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_set_state(nbody_ensemble* e, const double* x, const double* y,
+                                      const double* z, const double* m, const double* vx,
+                                      const double* vy, const double* vz) {
+  EN_TRY(ens_check(e));
+  const double* src[7] = {x, y, z, vx, vy, vz, m};
+  for (auto p : src)
+    if (!p) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null state array");
+  const size_t L = e->L;
+  double* dst[7] = {e->X, e->X + L, e->X + 2 * L, e->V, e->V + L, e->V + 2 * L, e->M};
+  long long off = 0;
+  for (int c = 0; c < e->C; ++c) {
+    for (int k = 0; k < 7; ++k)
+      EN_CUDA(cudaMemcpyAsync(dst[k] + e->row0[c], src[k] + off, sizeof(double) * e->n[c],
+                              cudaMemcpyHostToDevice, e->stream));
+    off += e->n[c];
+  }
+  EN_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * L, e->stream));
+  EN_TRY(launch_ens_pack(e));
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  e->have_derivs = false;
+  e->steps = 0;
+  if (e->tiles_per_item < 0) EN_TRY(ens_autotune(e));
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_get_state(nbody_ensemble* e, double* x, double* y, double* z,
+                                      double* vx, double* vy, double* vz) {
+  EN_TRY(ens_check(e));
+  const size_t L = e->L;
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  const double* src[6] = {e->X, e->X + L, e->X + 2 * L, e->V, e->V + L, e->V + 2 * L};
+  long long off = 0;
+  for (int c = 0; c < e->C; ++c) {
+    for (int k = 0; k < 6; ++k)
+      if (dst[k])
+        EN_CUDA(cudaMemcpyAsync(dst[k] + off, src[k] + e->row0[c], sizeof(double) * e->n[c],
+                                cudaMemcpyDeviceToHost, e->stream));
+    off += e->n[c];
+  }
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  return ens_status(e);
+}
+
+nbody_status nbody_ensemble_get_derivs(nbody_ensemble* e, double* ax, double* ay, double* az,
+                                       double* jx, double* jy, double* jz) {
+  EN_TRY(ens_check(e));
+  if (!e->have_derivs) return nbody_set_error(NBODY_ERR_STATE, "no derivatives yet");
+  const size_t L = e->L;
+  double* dst[6] = {ax, ay, az, jx, jy, jz};
+  long long off = 0;
+  for (int c = 0; c < e->C; ++c) {
+    for (int k = 0; k < 6; ++k)
+      if (dst[k])
+        EN_CUDA(cudaMemcpyAsync(dst[k] + off, e->D + k * L + e->row0[c], sizeof(double) * e->n[c],
+                                cudaMemcpyDeviceToHost, e->stream));
+    off += e->n[c];
+  }
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  return ens_status(e);
+}
+
+nbody_status nbody_ensemble_acc_jerk(nbody_ensemble* e) {
+  EN_TRY(ens_check(e));
+  return ens_eval_current(e);
+}
+
+nbody_status nbody_ensemble_step(nbody_ensemble* e, int nsteps) {
+  EN_TRY(ens_check(e));
+  if (nsteps < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "nsteps < 0");
+  if (!e->have_derivs) EN_TRY(ens_eval_current(e));
+  EN_TRY(ens_build_graph(e));
+  for (int k = 0; k < nsteps; ++k) EN_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  e->steps += nsteps;
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_synchronize(nbody_ensemble* e) {
+  EN_TRY(ens_check(e));
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  return ens_status(e);
+}
+
+nbody_status nbody_ensemble_energy(nbody_ensemble* e, double* T, double* U) {
+  EN_TRY(ens_check(e));
+  if (!T || !U) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null energy arrays");
+  ens_pack_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->cid, e->X, e->V,
+                                                                        e->M, e->jb64, nullptr);
+  ens_phi_kernel<<<e->n_blk, kBlock, 0, e->stream>>>(e->blk_cluster, e->blk_row, e->cl, e->jb64, e->phi);
+  ens_energy_sum_kernel<<<e->C, kBlock, 0, e->stream>>>(e->cl, e->V, e->M, e->phi, e->L, e->Tc, e->Uc);
+  EN_CUDA(cudaGetLastError());
+  EN_CUDA(cudaMemcpyAsync(T, e->Tc, sizeof(double) * e->C, cudaMemcpyDeviceToHost, e->stream));
+  EN_CUDA(cudaMemcpyAsync(U, e->Uc, sizeof(double) * e->C, cudaMemcpyDeviceToHost, e->stream));
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_info(nbody_ensemble* e, nbody_ensemble_info_t* out) {
+  EN_TRY(ens_check(e));
+  if (!out) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null info");
+  EN_CUDA(cudaStreamSynchronize(e->stream));
+  memset(out, 0, sizeof *out);
+  out->nclusters = e->C;
+  out->padded_rows = e->L;
+  out->items = e->n_items;
+  out->tiles_per_item = e->tiles_per_item;
+  out->grid = e->grid;
+  out->interactions_per_step = static_cast<double>(e->interactions);
+  out->steps = e->steps;
+  float ms = 0;
+  if (e->graph && cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]) == cudaSuccess) out->last_step_ms = ms;
+  cudaGetLastError();
+  return NBODY_OK;
+}
+
+nbody_status nbody_ensemble_get_stream(nbody_ensemble* e, void** stream) {
+  EN_TRY(ens_check(e));
+  if (!stream) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null stream out");
+  *stream = e->stream;
+  return NBODY_OK;
+}
+
+}  // extern "C"
