@@ -227,6 +227,51 @@ nbody_status nbody_ensemble_energy(nbody_ensemble* ens, double* T, double* U);
 nbody_status nbody_ensemble_info(nbody_ensemble* ens, nbody_ensemble_info_t* out);
 nbody_status nbody_ensemble_get_stream(nbody_ensemble* ens, void** stream);
 
+/* ---- adjoint (reverse-mode gradients) -----------------------------------------
+ * No reference counterpart.  Gradients of a scalar loss of the final positions
+ * and velocities of a fixed-dt Hermite-4 run with respect to the initial
+ * positions, velocities and masses.  The forward keeps the state every
+ * checkpoint_every steps; the backward recomputes each segment and runs the
+ * hand-written adjoint kernels (pair acc/jerk VJP in FP64, reverse corrector
+ * and predictor).  All arrays are float64 device pointers of n values on the
+ * adjoint's device; work is ordered on `stream` (cudaStream_t, NULL = legacy
+ * default stream); the calls return after their work completes. */
+typedef struct nbody_adjoint nbody_adjoint;
+typedef struct {
+  int n;
+  double eps2;
+  int precision;         /* forward pair loop: NBODY_FP64 or NBODY_MIXED     */
+  int device;
+  double dt;             /* fixed shared step (> 0)                          */
+  int nsteps;
+  int checkpoint_every;  /* >= 1                                             */
+} nbody_adjoint_config;
+
+nbody_status nbody_adjoint_create(nbody_adjoint** out, const nbody_adjoint_config* cfg);
+nbody_status nbody_adjoint_destroy(nbody_adjoint* adj);
+/* Runs nsteps from (x, v, m) and writes the final positions and velocities. */
+nbody_status nbody_adjoint_forward(nbody_adjoint* adj, const double* x, const double* y,
+                                   const double* z, const double* m, const double* vx,
+                                   const double* vy, const double* vz, double* x1, double* y1,
+                                   double* z1, double* vx1, double* vy1, double* vz1,
+                                   void* stream);
+/* Given dL/d(final x, v), writes dL/d(initial x, v) and dL/dm.  Needs the
+ * preceding nbody_adjoint_forward. */
+nbody_status nbody_adjoint_backward(nbody_adjoint* adj, const double* gx, const double* gy,
+                                    const double* gz, const double* gvx, const double* gvy,
+                                    const double* gvz, double* gx0, double* gy0, double* gz0,
+                                    double* gvx0, double* gvy0, double* gvz0, double* gm,
+                                    void* stream);
+/* One pair VJP: given adjoints (abar, jbar) of acc and jerk at state (x, v, m),
+ * writes (xbar, vbar, mbar) = the transposed Jacobian applied to them. */
+nbody_status nbody_adjoint_vjp_acc_jerk(nbody_adjoint* adj, const double* x, const double* y,
+                                        const double* z, const double* m, const double* vx,
+                                        const double* vy, const double* vz, const double* abx,
+                                        const double* aby, const double* abz, const double* jbx,
+                                        const double* jby, const double* jbz, double* gx,
+                                        double* gy, double* gz, double* gvx, double* gvy,
+                                        double* gvz, double* gm, void* stream);
+
 /* ---- initial conditions (host, deterministic) ------------------------------
  * Plummer sphere in Henon units (G = M = 1, E = -1/4), equal masses 1/n,
  * centred on the origin in position and velocity; sampled by the

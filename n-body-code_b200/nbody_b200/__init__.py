@@ -6,9 +6,10 @@ C-ABI in include/nbody_cuda.h); this package only marshals arguments.
 from ._lib import LIB_PATH, NBodyError, header_functions, load
 from .engine import (Engine, FIELDS, force_calculation, measure_peaks, plummer, reference_ic,
                      release_force_cache)
+from .adjoint import Adjoint, hermite_rollout
 from .ensemble import Ensemble, plummer_ensemble
 
 __all__ = [
-    "Engine", "Ensemble", "plummer_ensemble", "FIELDS", "LIB_PATH", "NBodyError", "force_calculation", "header_functions", "load",
+    "Adjoint", "Engine", "Ensemble", "hermite_rollout", "plummer_ensemble", "FIELDS", "LIB_PATH", "NBodyError", "force_calculation", "header_functions", "load",
     "measure_peaks", "plummer", "reference_ic", "release_force_cache",
 ]

@@ -31,6 +31,12 @@
 // New (no reference counterpart), used as checkers for the GPU engine:
 //   orc_force_rows_fp64   direct j-sum for selected i-rows (large-N sampling)
 //   orc_potential_rows    per-row potential phi_i = -sum_{j!=i} m_j/r_ij
+//   orc_force_jvp         tangent (forward-mode derivative) of the pair
+//                         acc/jerk along a direction (dx, dv, dm)
+//   orc_hermite_tlm       tangent-linear model of the fixed-dt Hermite run:
+//                         the trajectory of orc_hermite_fixed and its
+//                         directional derivative, the reference for the
+//                         adjoint (reverse-mode) gradients
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -402,6 +408,86 @@ void orc_hermite_fixed(int n, double eps2, double dt, int nsteps, int precision,
   memcpy(vz, V + 2 * n, n * sizeof(double));
   memcpy(derivs, A, 6 * (size_t)n * sizeof(double));
   if (dt_next_out) *dt_next_out = dtn;
+}
+
+// Directional derivative of (acc, jerk) at (x, v, m) along (dx, dv, dm); direct
+// j-sum with the libm 1/sqrt.  Arrays are [3][n] blocks (x, v, dx, dv, and
+// the outputs da, dj); m and dm have n values.
+void orc_force_jvp(int n, double eps2, const double* x, const double* v, const double* m,
+                   const double* dx, const double* dv, const double* dm, double* da, double* dj) {
+  for (int i = 0; i < n; ++i) {
+    double A[3] = {0, 0, 0}, J[3] = {0, 0, 0};
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      double r[3], u[3], dr[3], du[3];
+      for (int c = 0; c < 3; ++c) {
+        r[c] = x[c * n + j] - x[c * n + i];
+        u[c] = v[c * n + j] - v[c * n + i];
+        dr[c] = dx[c * n + j] - dx[c * n + i];
+        du[c] = dv[c * n + j] - dv[c * n + i];
+      }
+      const double s = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + eps2;
+      const double ds = 2.0 * (r[0] * dr[0] + r[1] * dr[1] + r[2] * dr[2]);
+      const double y = 1.0 / std::sqrt(s);
+      const double q = y * y * y;
+      const double dq = -1.5 * q * ds / s;
+      const double w = r[0] * u[0] + r[1] * u[1] + r[2] * u[2];
+      const double dw = dr[0] * u[0] + dr[1] * u[1] + dr[2] * u[2] + r[0] * du[0] + r[1] * du[1] + r[2] * du[2];
+      const double c3 = -3.0 * w / s;
+      const double dc = -3.0 * (dw / s - w * ds / (s * s));
+      for (int c = 0; c < 3; ++c) {
+        A[c] += dm[j] * q * r[c] + m[j] * dq * r[c] + m[j] * q * dr[c];
+        const double g = u[c] + c3 * r[c];
+        J[c] += dm[j] * q * g + m[j] * dq * g + m[j] * q * (du[c] + dc * r[c] + c3 * dr[c]);
+      }
+    }
+    for (int c = 0; c < 3; ++c) {
+      da[c * n + i] = A[c];
+      dj[c * n + i] = J[c];
+    }
+  }
+}
+
+// Fixed-dt Hermite run (the trajectory of orc_hermite_fixed, FP64) together
+// with its tangent along (dx0, dv0, dm).  X, V, DX, DV are [3][n] blocks,
+// in/out; m, dm have n values.  The corrector tangent uses its expanded
+// linear form x1 = xp - 0.15 h^2 (a0 - a1) - h^3 (7/60 j0 + 1/30 j1),
+// v1 = vp - 0.5 h (a0 - a1) - h^2 (5/12 j0 + 1/12 j1).
+void orc_hermite_tlm(int n, double eps2, double h, int nsteps, double* X, double* V,
+                     const double* m, double* DX, double* DV, const double* dm) {
+  const size_t N3 = 3 * (size_t)n;
+  std::vector<double> d0(6 * (size_t)n), d1(6 * (size_t)n), a2(N3), a3(N3);
+  std::vector<double> t0(6 * (size_t)n), t1(6 * (size_t)n);  // tangents of (a, j)
+  double* A = d0.data();
+  double* B = d1.data();
+  double* TA = t0.data();
+  double* TB = t1.data();
+  orc_force_fp64(n, eps2, X, X + n, X + 2 * n, m, V, V + n, V + 2 * n, A, A + n, A + 2 * n,
+                 A + 3 * n, A + 4 * n, A + 5 * n);
+  orc_force_jvp(n, eps2, X, V, m, DX, DV, dm, TA, TA + 3 * n);
+  const double h2 = h * h, h3 = h2 * h;
+  for (int s = 0; s < nsteps; ++s) {
+    for (size_t k = 0; k < N3; ++k) {  // tangent predictor
+      const double tx = DX[k] + h * DV[k] + 0.5 * h2 * TA[k] + (h3 / 6.0) * TA[N3 + k];
+      const double tv = DV[k] + h * TA[k] + 0.5 * h2 * TA[N3 + k];
+      DX[k] = tx;
+      DV[k] = tv;
+    }
+    orc_predict(n, h, X, X + n, X + 2 * n, V, V + n, V + 2 * n, A, A + n, A + 2 * n, A + 3 * n,
+                A + 4 * n, A + 5 * n);
+    orc_force_fp64(n, eps2, X, X + n, X + 2 * n, m, V, V + n, V + 2 * n, B, B + n, B + 2 * n,
+                   B + 3 * n, B + 4 * n, B + 5 * n);
+    orc_force_jvp(n, eps2, X, V, m, DX, DV, dm, TB, TB + 3 * n);
+    for (size_t k = 0; k < N3; ++k) {  // tangent corrector
+      const double dA = TA[k] - TB[k];
+      DX[k] += -0.15 * h2 * dA - h3 * ((7.0 / 60.0) * TA[N3 + k] + (1.0 / 30.0) * TB[N3 + k]);
+      DV[k] += -0.5 * h * dA - h2 * ((5.0 / 12.0) * TA[N3 + k] + (1.0 / 12.0) * TB[N3 + k]);
+    }
+    orc_snapcrackle(n, h, A, A + 3 * n, B, B + 3 * n, a2.data(), a3.data());
+    orc_correct(n, h, X, V, a2.data(), a3.data());
+    std::swap(A, B);
+    std::swap(TA, TB);
+  }
 }
 
 }  // extern "C"

@@ -80,6 +80,8 @@ def lib():
         L.orc_initialize.argtypes = [C.c_int] + [C.c_double] * 5 + [_dp] * 7
         L.orc_hermite_fixed.argtypes = ([C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
                                         + [_dp] * 8 + [_dp])
+        L.orc_force_jvp.argtypes = [C.c_int, C.c_double] + [_dp] * 8
+        L.orc_hermite_tlm.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int] + [_dp] * 6
         _lib = L
     return _lib
 
@@ -239,3 +241,30 @@ def ref_hermite_fixed(state: dict, dt: float, nsteps: int, f32: bool = False):
     ref(f32).ref_hermite_fixed(x.size, dt, nsteps, *map(_p, (x, y, z, m, vx, vy, vz)),
                                *[_p(d[k]) for k in range(6)], C.byref(dtn))
     return dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz), d, dtn.value
+
+
+def _blk(s, keys):
+    return np.ascontiguousarray(np.stack([np.asarray(s[k], dtype=np.float64) for k in keys]))
+
+
+def force_jvp(state: dict, eps2: float, dx, dv, dm):
+    """Tangent of (acc, jerk) along (dx (3,n), dv (3,n), dm (n,)); returns (da, dj)."""
+    X = _blk(state, ("x", "y", "z")); V = _blk(state, ("vx", "vy", "vz"))
+    m = np.ascontiguousarray(state["m"], dtype=np.float64)
+    dx = np.ascontiguousarray(dx, dtype=np.float64); dv = np.ascontiguousarray(dv, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    n = m.size
+    da = np.zeros((3, n)); dj = np.zeros((3, n))
+    lib().orc_force_jvp(n, eps2, _p(X), _p(V), _p(m), _p(dx), _p(dv), _p(dm), _p(da), _p(dj))
+    return da, dj
+
+
+def hermite_tlm(state: dict, eps2: float, dt: float, nsteps: int, dx, dv, dm):
+    """Fixed-dt FP64 run and its tangent: returns (X1 (3,n), V1 (3,n), DX1, DV1)."""
+    X = _blk(state, ("x", "y", "z")); V = _blk(state, ("vx", "vy", "vz"))
+    m = np.ascontiguousarray(state["m"], dtype=np.float64)
+    DX = np.array(dx, dtype=np.float64, copy=True, order="C")
+    DV = np.array(dv, dtype=np.float64, copy=True, order="C")
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    lib().orc_hermite_tlm(m.size, eps2, dt, nsteps, _p(X), _p(V), _p(m), _p(DX), _p(DV), _p(dm))
+    return X, V, DX, DV
