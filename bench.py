@@ -21,12 +21,20 @@ system on its own GPU with no data exchange; value = ranks x N^2 / max time.
 """
 from __future__ import annotations
 
+import os
+
+# The reference CPU force loop keeps OpenMP private copies of its six output
+# arrays on each thread's stack (array-section reductions, src/kernel.cpp:1180):
+# 48 bytes per body per thread.  Worker stacks are sized before anything loads
+# libgomp; the calling thread gets its own large stack (cpu_call below).
+os.environ.setdefault("OMP_STACKSIZE", "256M")
+
 import argparse
 import json
-import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -53,6 +61,7 @@ def parse():
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--tune", action="store_true", help="autotune pair-kernel tiling first")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the main arm only (no peaks, e2e, CPU baseline): the profiling case")
     ap.add_argument("--ensemble", action="store_true",
@@ -60,7 +69,9 @@ def parse():
                          "[256, 8192], eps = 4/N, dt = 1/512, vs one launch per cluster")
     ap.add_argument("--clusters", type=int, default=512)
     ap.add_argument("--time-units", type=float, default=0.0,
-                    help="ensemble: also integrate this many N-body time units and report |dE/E|")
+                    help="also integrate this many N-body time units (untimed) and report |dE/E|")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="report the mixed path's per-body acc/jerk error against FP64 at t = 0")
     return ap.parse_args()
 
 
@@ -135,6 +146,7 @@ def traffic_per_launch(precision):
 def run_arm(a, precision, state, torch, dist, rank, world, dev):
     import nbody_b200 as nb
     n = a.n
+    clk = ClockSampler(dev).__enter__()  # sampling starts before the warm-up so the timed region is covered
     e = nb.Engine(n, eps2=a.eps ** 2, precision=precision, device=dev, dt=a.dt, tune=a.tune)
     e.set_state(state)
     e.force_calculation()
@@ -149,7 +161,7 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    with torch.cuda.stream(stream), ClockSampler(dev) as clk:
+    with torch.cuda.stream(stream):
         for k in range(a.steps):
             flush.zero_()                       # evict L2 between timed steps
             starts[k].record(stream)
@@ -159,10 +171,19 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
             t = e.timers()                      # graph-internal events of this step
             pred_ms.append(t["pred_ms"]); pair_ms.append(t["eval_ms"]); corr_ms.append(t["corr_ms"])
     torch.cuda.synchronize(dev)
+    clk.__exit__(None, None, None)
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(t) for s, t in zip(starts, ends)]
     tm = e.timers()
+    if a.time_units > 0:  # carry on (untimed) to the requested model time
+        rest = int(round(a.time_units / a.dt)) - a.warmup - a.steps
+        while rest > 0:
+            k = min(rest, 256)
+            e.timestepping(k)
+            e.synchronize()
+            rest -= k
+    t_end = e.timers()["t"]
     T1, U1 = e.energy()
     de = abs((T1 + U1) - (T0 + U0)) / abs(T0 + U0)
     e.close()
@@ -172,6 +193,7 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
         "pred_ms": float(np.mean(pred_ms)),
         "corr_ms": float(np.mean(corr_ms)),
         "dE_over_E": de,
+        "t_end": t_end,
         "E0": T0 + U0,
         "tiling": {k: tm[k] for k in ("threads", "i_per_thread", "j_tile", "split_j")},
         "clocks": clk.summary(),
@@ -216,6 +238,28 @@ def run_e2e(a, precision, state, torch, steps):
 # ---------------------------------------------------------------------------
 # CPU: the reference's own code (oracle/_ref) or, if absent, the oracle port
 # ---------------------------------------------------------------------------
+def cpu_call(fn, *args):
+    """Runs fn on a thread with a 1 GiB stack (the OpenMP master thread of the
+    reference's force loop needs 48 bytes of stack per body)."""
+    out = {}
+
+    def body():
+        try:
+            out["r"] = fn(*args)
+        except BaseException as exc:  # re-raised in the caller
+            out["e"] = exc
+    old = threading.stack_size(1 << 30)
+    try:
+        th = threading.Thread(target=body)
+        th.start()
+        th.join()
+    finally:
+        threading.stack_size(old)
+    if "e" in out:
+        raise out["e"]
+    return out.get("r")
+
+
 def cpu_reference_steps(a, state, nsteps, seconds_per_step):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -267,8 +311,8 @@ def cpu_port_steps(a, state, nsteps, seconds_per_step):
 
 
 def cpu_baseline(a, state):
-    r = cpu_reference_steps(a, state, 3, a.cpu_sample_seconds / 3) or \
-        cpu_port_steps(a, state, 3, a.cpu_sample_seconds / 3)
+    r = cpu_call(cpu_reference_steps, a, state, 3, a.cpu_sample_seconds / 3) or \
+        cpu_call(cpu_port_steps, a, state, 3, a.cpu_sample_seconds / 3)
     v = a.n * a.n / float(np.mean(r["per_step_s"])) / 1e9
     return {"value": v, "unit": "Gint/s", "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
 
@@ -289,9 +333,9 @@ def main_reference(a):
     state = nb.plummer(a.n, a.seed)
     total = a.steps + a.warmup
     per_step_budget = min(2.0, max(0.2, 150.0 / max(total, 1)))
-    r = cpu_reference_steps(a, state, total, per_step_budget)
+    r = cpu_call(cpu_reference_steps, a, state, total, per_step_budget)
     if r is None:
-        r = cpu_port_steps(a, state, total, per_step_budget)
+        r = cpu_call(cpu_port_steps, a, state, total, per_step_budget)
     timed = r["per_step_s"][a.warmup:]
     s = float(np.mean(timed))
     v = a.n * a.n / s / 1e9
@@ -441,11 +485,28 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    accuracy = None
+    if a.accuracy and rank == 0:
+        d = {}
+        for prec in ("fp64", "mixed"):
+            with nb.Engine(a.n, eps2=a.eps ** 2, precision=prec, device=dev, dt=a.dt) as e:
+                e.set_state(state)
+                e.force_calculation()
+                d[prec] = e.get_derivs()
+
+        def rel(blk):
+            num = np.sqrt(((d["mixed"][blk] - d["fp64"][blk]) ** 2).sum(0))
+            return num / np.sqrt((d["fp64"][blk] ** 2).sum(0))
+        ea, ej = rel(slice(0, 3)), rel(slice(3, 6))
+        accuracy = {"acc_rel_err_vs_fp64": {"median": float(np.median(ea)), "p99": float(np.quantile(ea, 0.99)),
+                                            "max": float(ea.max())},
+                    "jerk_rel_err_vs_fp64": {"median": float(np.median(ej)), "p99": float(np.quantile(ej, 0.99)),
+                                             "max": float(ej.max())}}
     ms = max_over_ranks(main_arm["ms_per_step"])
     pair_ms = max_over_ranks(main_arm["pair_ms"])
     e2e = run_e2e(a, a.precision, state, torch, max(3, min(a.steps, 20)))
     e2e["value"] = e2e["value"] * world
-    cpu = cpu_baseline(a, state) if (rank == 0 and world == 1) else None
+    cpu = cpu_baseline(a, state) if (rank == 0 and world == 1 and not a.no_cpu_baseline) else None
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -479,7 +540,8 @@ def main():
         "clocks": main_arm["clocks"],
         "phases_ms": {"pred": main_arm["pred_ms"], "eval": main_arm["pair_ms"], "corr": main_arm["corr_ms"]},
         "tiling": main_arm["tiling"],
-        "energy_error": {a.precision: main_arm["dE_over_E"]},
+        "energy_error": {a.precision: main_arm["dE_over_E"], "t_end": main_arm["t_end"]},
+        "accuracy_t0": accuracy,
         "peaks_measured": peaks,
     }
     if other is not None:
