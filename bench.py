@@ -318,6 +318,26 @@ def cpu_baseline(a, state):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks_fn(world, dist, device):
+    """x -> max of x over all ranks (all-reduce MAX on `device`; NCCL on GPUs,
+    gloo on CPU)."""
+    if world == 1:
+        return lambda x: x
+    import torch
+
+    def f(x):
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return f
+
+
+def replica_value(world, interactions_per_replica, ms_per_step):
+    """Whole-job G interactions/s of `world` independent replicas timed at the
+    slowest rank's step time."""
+    return world * interactions_per_replica / (ms_per_step * 1e-3) / 1e9
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -478,12 +498,7 @@ def main():
     if not a.no_fp64_arm:
         other = run_arm(a, other_prec, state, torch, dist, rank, world, dev)
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = max_over_ranks_fn(world, dist, f"cuda:{dev}")
 
     accuracy = None
     if a.accuracy and rank == 0:
@@ -513,7 +528,7 @@ def main():
         dist.destroy_process_group()
         return 0
     inter = float(a.n) * a.n
-    value = world * inter / (ms * 1e-3) / 1e9
+    value = replica_value(world, inter, ms)
 
     def roofline(arm, prec):
         peak = peaks["fp32_tflops"] if prec == "mixed" else peaks["fp64_tflops"]
@@ -545,7 +560,7 @@ def main():
         "peaks_measured": peaks,
     }
     if other is not None:
-        ov = world * inter / (max_over_ranks(other["ms_per_step"]) * 1e-3) / 1e9
+        ov = replica_value(world, inter, max_over_ranks(other["ms_per_step"]))
         line[other_prec] = {"value": ov, "ms_per_step": other["ms_per_step"], "pair_ms": other["pair_ms"],
                             "roofline": roofline(other, other_prec), "tiling": other["tiling"],
                             "clocks": other["clocks"]}

@@ -306,6 +306,12 @@ typedef struct {
 } nbody_peaks;
 nbody_status nbody_measure_peaks(int device, nbody_peaks* out);
 
+/* Failure-path self-test: one kernel waits on a shared-memory barrier that
+ * never completes; its bounded wait gives up after limit_ms (0 < limit_ms <=
+ * 2000) and reports through the device status word.  Returns
+ * NBODY_ERR_TIMEOUT when the path works (the context stays usable). */
+nbody_status nbody_selftest_bounded_wait(int device, double limit_ms);
+
 #ifdef __cplusplus
 }
 #endif

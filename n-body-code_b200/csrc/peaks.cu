@@ -11,8 +11,25 @@
 #include <cstring>
 
 #include "../../include/nbody_cuda.h"
+#include "errors.h"
+#include "tma.cuh"
 
 namespace {
+
+// One CTA waits on an mbarrier that nothing ever arrives on: phase 0 never
+// completes, so the bounded wait gives up after limit_ns and the CTA records
+// the timeout in the status word - the same path every pipeline wait takes.
+__global__ void selftest_wait_kernel(uint64_t limit_ns, int* status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    nbody::mbar_init(&bar, 1);
+    nbody::mbar_init_fence();
+  }
+  __syncthreads();
+  const bool ok = nbody::mbar_wait_for(&bar, 0, limit_ns);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) nbody::report_status(status, nbody::kKernelTimeout);
+}
+
 
 constexpr int kChains = 8;
 constexpr int kThreads = 256;
@@ -146,4 +163,23 @@ extern "C" nbody_status nbody_measure_peaks(int device, nbody_peaks* out) {
   cudaEventDestroy(b);
   cudaFree(sink);
   return cudaGetLastError() == cudaSuccess ? NBODY_OK : NBODY_ERR_CUDA;
+}
+
+extern "C" nbody_status nbody_selftest_bounded_wait(int device, double limit_ms) {
+  if (!(limit_ms > 0 && limit_ms <= 2000))
+    return nbody_set_error(NBODY_ERR_INVALID_ARG, "limit_ms = %g outside (0, 2000]", limit_ms);
+  if (cudaSetDevice(device) != cudaSuccess) return nbody_set_error(NBODY_ERR_NO_DEVICE, "device %d", device);
+  int* st = nullptr;
+  if (cudaMalloc(&st, sizeof(int)) != cudaSuccess) return nbody_set_error(NBODY_ERR_OOM, "status word");
+  cudaMemset(st, 0, sizeof(int));
+  selftest_wait_kernel<<<1, 32>>>(static_cast<uint64_t>(limit_ms * 1e6), st);
+  int h = -1;
+  const cudaError_t e1 = cudaDeviceSynchronize();
+  const cudaError_t e2 = cudaMemcpy(&h, st, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(st);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return nbody_set_error(NBODY_ERR_CUDA, "self-test kernel: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  if (h == nbody::kKernelTimeout)
+    return nbody_set_error(NBODY_ERR_TIMEOUT, "in-kernel wait gave up after %.3g ms (self-test)", limit_ms);
+  return NBODY_OK;
 }

@@ -66,14 +66,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 
-// Waits for phase `parity` of `bar` to complete; false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Waits for phase `parity` of `bar` to complete; false after limit_ns.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (uint32_t k = 1;; ++k) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((k & 255u) == 0 && global_ns() - t0 > kWaitLimitNs) return false;
+    if ((k & 255u) == 0 && global_ns() - t0 > limit_ns) return false;
   }
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, kWaitLimitNs);
 }
 
 __device__ __forceinline__ void report_status(int* status, int code) {
