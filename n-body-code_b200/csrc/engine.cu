@@ -75,25 +75,25 @@ struct PairKernel {
   int fmt;      // RecordFormat of the j-records it reads
   const void* fn;
   size_t smem;  // dynamic shared memory: two j-tile buffers (+ FP64 accumulators)
-  int acc_smem = 0, junroll = 2;
+  int acc_smem = 0, junroll = 2, minb = 1;
 };
 
-template <int NT, int IPT, int TJ, int JU = 2>
+template <int NT, int IPT, int TJ, int JU = 2, int MINB = 1>
 PairKernel make_fp64() {
   return {NBODY_FP64, NT, IPT, TJ, kRecF64,
-          reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ, JU>), 2 * TJ * sizeof(JBody64),
-          0, JU};
+          reinterpret_cast<const void*>(&pair_fp64_kernel<NT, IPT, TJ, JU, MINB>),
+          2 * TJ * sizeof(JBody64), 0, JU, MINB};
 }
 template <int NT, int IPT, int TJ>
 PairKernel make_mixed() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecF32,
           reinterpret_cast<const void*>(&pair_mixed_kernel<NT, IPT, TJ>), 2 * TJ * sizeof(JBody32)};
 }
-template <int NT, int IPT, int TJ, int ACC = 0, int JU = 2>
+template <int NT, int IPT, int TJ, int ACC = 0, int JU = 2, int MINB = 1>
 PairKernel make_mixed_x2() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecX2,
-          reinterpret_cast<const void*>(&pair_mixed_x2_kernel<NT, IPT, TJ, ACC, JU>),
-          2 * TJ * sizeof(JBodyX2) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU};
+          reinterpret_cast<const void*>(&pair_mixed_x2_kernel<NT, IPT, TJ, ACC, JU, MINB>),
+          2 * TJ * sizeof(JBodyX2) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU, MINB};
 }
 
 // The first entry of each shape/variant is the one explicit tilings select;
@@ -103,10 +103,13 @@ const std::vector<PairKernel>& registry() {
       make_fp64<128, 2, 128, 1>(),  make_fp64<128, 2, 128, 2>(),  make_fp64<128, 1, 128, 4>(),
       make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
       make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
+      make_fp64<128, 2, 128, 1, 6>(), make_fp64<128, 2, 64, 1, 6>(), make_fp64<128, 1, 128, 4, 8>(),
       // packed pairs, FP64 accumulators in shared memory (default)
       make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
       make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
       make_mixed_x2<128, 2, 128, 1, 1>(),
+      make_mixed_x2<128, 4, 64, 1, 1, 5>(), make_mixed_x2<128, 4, 64, 1, 1, 6>(),
+      make_mixed_x2<128, 4, 64, 1, 1>(),    make_mixed_x2<64, 4, 64, 1, 1, 10>(),
       // packed pairs, FP64 accumulators in registers
       make_mixed_x2<128, 4, 128, 0, 2>(), make_mixed_x2<128, 2, 128, 0, 2>(),
       make_mixed_x2<256, 2, 128, 0, 2>(), make_mixed_x2<64, 4, 128, 0, 2>(),
@@ -316,8 +319,8 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
       float ms = 0.f;
       NB_CUDA(cudaEventElapsedTime(&ms, a, b));
       if (getenv("NBODY_TUNE_VERBOSE"))
-        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d split=%d  %.4f ms\n",
-                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, s, ms / 3);
+        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d minb=%d split=%d  %.4f ms\n",
+                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, k.minb, s, ms / 3);
       if (ms < best) {
         best = ms;
         best_idx = static_cast<int>(idx);
