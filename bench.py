@@ -68,6 +68,9 @@ def parse():
                     help="batched-ensemble workload: Plummer clusters (seed 3), N log-uniform in "
                          "[256, 8192], eps = 4/N, dt = 1/512, vs one launch per cluster")
     ap.add_argument("--clusters", type=int, default=512)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="gradient workload: Plummer N=4096 (seed 4), eps=1e-2, dt=1/256, 256 steps, "
+                         "checkpoint every 16; forward and backward times")
     ap.add_argument("--time-units", type=float, default=0.0,
                     help="also integrate this many N-body time units (untimed) and report |dE/E|")
     ap.add_argument("--accuracy", action="store_true",
@@ -466,12 +469,57 @@ def main_ensemble(a):
     return 0
 
 
+def main_adjoint(a):
+    """Checkpointed adjoint: time of the forward run and of the backward
+    sweep (segment recompute + reverse steps) on the torch stream."""
+    import torch
+    import nbody_b200 as nb
+    n, eps2, dt, nsteps, k = 4096, 1e-4, 1.0 / 256, 256, 16
+    s = nb.plummer(n, 4)
+    rng = np.random.default_rng(4)
+    sel = torch.tensor(np.sort(rng.choice(n, 64, replace=False)), device="cuda")
+    X = torch.tensor(np.stack([s["x"], s["y"], s["z"]]), dtype=torch.float64, device="cuda")
+    V = torch.tensor(np.stack([s["vx"], s["vy"], s["vz"]]), dtype=torch.float64, device="cuda")
+    m = torch.tensor(s["m"], dtype=torch.float64, device="cuda")
+    out = {"metric": "checkpointed adjoint of a fixed-dt Hermite-4 run (gradients w.r.t. x0, v0, m)",
+           "config": {"workload": "Plummer N=4096 seed 4, eps=1e-2, dt=1/256, 256 steps, checkpoint 16, "
+                                  "loss = sum |x_final - target|^2 over 64 seeded bodies"},
+           "unit": "ms", "higher_is_better": False}
+    for prec in ("fp64", "mixed"):
+        adj = nb.Adjoint(n, eps2, dt, nsteps, k, precision=prec)
+        fw, bw = [], []
+        for rep in range(a.warmup + a.steps):
+            x0 = X.clone().requires_grad_()
+            v0 = V.clone().requires_grad_()
+            mm = m.clone().requires_grad_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            x1, v1 = nb.hermite_rollout(x0, v0, mm, eps2, dt, nsteps, k, prec, adjoint=adj)
+            e1.record()
+            target = x1.detach()[:, sel] + 1e-3
+            ((x1[:, sel] - target) ** 2).sum().backward()
+            e2.record()
+            torch.cuda.synchronize()
+            if rep >= a.warmup:
+                fw.append(e0.elapsed_time(e1))
+                bw.append(e1.elapsed_time(e2))
+        adj.close()
+        inter = float(n) * n * (nsteps + 1)
+        out[prec] = {"forward_ms": float(np.mean(fw)), "backward_ms": float(np.mean(bw)),
+                     "forward_Gint_s": inter / (np.mean(fw) * 1e-3) / 1e9}
+    out["value"] = out["fp64"]["forward_ms"] + out["fp64"]["backward_ms"]
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return main_reference(a)
     if a.ensemble:
         return main_ensemble(a)
+    if a.adjoint:
+        return main_adjoint(a)
     import torch
     world, rank, local = dist_setup()
     dist = None
