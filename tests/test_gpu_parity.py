@@ -243,3 +243,17 @@ def test_device_pointer_entry_matches_engine():
     got = torch.stack(out).cpu().numpy()
     ea, ej = derivs_rel(got, ref)
     assert ea <= 1e-13 and ej <= 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_max_size_sampled_rows(precision):
+    """N = 2^20: indexing at scale (padded arrays of ~10^6 rows, 64-bit
+    partial offsets); sampled rows against the oracle's direct sums."""
+    n, eps2 = 1 << 20, 1e-4
+    s = nb.plummer(n, seed=6)
+    d = engine_derivs(s, eps2, precision=precision)
+    rows = np.array([0, 1, 12345, n // 2, n - 2, n - 1])
+    ref = O.force_rows(s, eps2, rows)
+    ea, ej = derivs_rel(d[:, rows], ref)
+    tol = TOL_FP64 if precision == "fp64" else 1e-5
+    assert ea <= tol and ej <= 10 * tol, (precision, ea, ej)
