@@ -156,7 +156,9 @@ nbody_status nbody_force_calculation_release(void);
  * Same physics on caller-owned device arrays (float64, n each, on the
  * engine's device); work is ordered on `stream` (cudaStream_t, NULL = the
  * engine's stream).  eng supplies eps2, precision, tiling and scratch; n must
- * be <= the engine's n. */
+ * be <= the engine's n.  It reuses the engine's j-record and partial-sum
+ * buffers, so an engine used this way should not be stepping at the same time
+ * (between a nbody_predict and its nbody_eval_predicted, say). */
 nbody_status nbody_acc_jerk_device(nbody_engine* eng, int n, const double* x, const double* y,
                                    const double* z, const double* m, const double* vx,
                                    const double* vy, const double* vz, double* ax, double* ay,

@@ -58,9 +58,8 @@ constexpr int kVjpNT = 128, kVjpTile = 64;
 
 // Row block of the pair VJP: one row per thread.
 struct RowsVJP {
-  static constexpr int NT = kVjpNT, ROWS = kVjpNT, TJ = kVjpTile;
+  static constexpr int TJ = kVjpTile;
   using JB = JAdj;
-  static constexpr size_t kExtraSmem = 0;
   double x, y, z, m, u, v, w, ax, ay, az, bx, by, bz;
   double rpk[3], upk[3], rkp[3], ukp[3], mb;
   double eps2;

@@ -171,6 +171,7 @@ struct nbody_engine {
   int p_splits = 0;
   JBody64* jb64 = nullptr;
   void* jb32 = nullptr;  // mixed records: JBody32 or JBodyX2 (sized for the larger)
+  JBody64* jbe = nullptr;  // records of the energy diagnostic (never a pair kernel's input)
   StepCtl* ctl = nullptr;
   double* partial = nullptr;  // reduction scratch: ld / 256 + 1 doubles + 4 scalars
   int* status = nullptr;
@@ -342,9 +343,8 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
 // Tiling for `rows` i-rows: explicit config, else tuned, else heuristic.
 nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
   const nbody_config& c = e->cfg;
-  const bool fp64 = c.precision == NBODY_FP64;
   int nt = c.threads ? c.threads : 128;
-  int ipt = c.i_per_thread ? c.i_per_thread : (fp64 ? 2 : 4);
+  int ipt = c.i_per_thread ? c.i_per_thread : 2;
   int tj = c.j_tile ? c.j_tile : 128;
   const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, c.pair_variant);
   if (!k)
@@ -557,6 +557,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
     e->M = e->state + 6 * ld;
     e->D = e->state + 7 * ld;
     NB_CUDA(cudaMalloc(&e->jb64, sizeof(JBody64) * ld));
+    NB_CUDA(cudaMalloc(&e->jbe, sizeof(JBody64) * ld));
     if (cfg->precision == NBODY_MIXED) NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyX2) * ld));
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
     NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 + 8)));
@@ -583,6 +584,7 @@ nbody_status nbody_destroy(nbody_engine* e) {
   cudaFree(e->P);
   cudaFree(e->jb64);
   cudaFree(e->jb32);
+  cudaFree(e->jbe);
   cudaFree(e->ctl);
   cudaFree(e->partial);
   cudaFree(e->status);
@@ -687,9 +689,9 @@ nbody_status nbody_energy(nbody_engine* e, int ref_compat, double* T, double* U)
   double* scal = e->partial + nb;  // two result slots after the partials
   kinetic_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->V, e->M, e->partial);
   sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal);
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, kRecF64));
+  pack_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, own_inputs(e), e->jbe, nullptr, nullptr);
   potential_kernel<kBlockO1><<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->cfg.eps2,
-                                                             ref_compat ? 1 : 0, e->jb64, e->partial);
+                                                             ref_compat ? 1 : 0, e->jbe, e->partial);
   sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal + 1);
   NB_CUDA(cudaGetLastError());
   double h[2];
