@@ -40,6 +40,7 @@
 #include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
+#include "trace.h"
 
 using namespace nbody;
 
@@ -439,6 +440,7 @@ nbody_status nbody_adjoint_forward(nbody_adjoint* a, const double* x, const doub
                                    const double* m, const double* vx, const double* vy,
                                    const double* vz, double* x1, double* y1, double* z1, double* vx1,
                                    double* vy1, double* vz1, void* stream) {
+  TraceRange trace_("nbody_adjoint_forward");
   if (!a) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null adjoint");
   const void* ptrs[13] = {x, y, z, m, vx, vy, vz, x1, y1, z1, vx1, vy1, vz1};
   for (auto p : ptrs)
@@ -473,6 +475,7 @@ nbody_status nbody_adjoint_backward(nbody_adjoint* a, const double* gx, const do
                                     const double* gvz, double* gx0, double* gy0, double* gz0,
                                     double* gvx0, double* gvy0, double* gvz0, double* gm,
                                     void* stream) {
+  TraceRange trace_("nbody_adjoint_backward");
   if (!a) return nbody_set_error(NBODY_ERR_INVALID_ARG, "null adjoint");
   if (!a->have_forward) return nbody_set_error(NBODY_ERR_STATE, "backward before forward");
   const void* ptrs[13] = {gx, gy, gz, gvx, gvy, gvz, gx0, gy0, gz0, gvx0, gvy0, gvz0, gm};

@@ -32,6 +32,7 @@
 #include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
+#include "trace.h"
 
 using namespace nbody;
 
@@ -596,6 +597,7 @@ nbody_status nbody_destroy(nbody_engine* e) {
 nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, const double* z,
                              const double* m, const double* vx, const double* vy,
                              const double* vz) {
+  TraceRange trace_("nbody_set_state");
   NB_TRY(check_engine(e));
   const double* src[7] = {x, y, z, vx, vy, vz, m};
   for (auto p : src)
@@ -623,6 +625,7 @@ nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, 
 
 nbody_status nbody_get_state(nbody_engine* e, double* x, double* y, double* z, double* vx,
                              double* vy, double* vz) {
+  TraceRange trace_("nbody_get_state");
   NB_TRY(need_state(e));
   const size_t ld = e->ld, b = sizeof(double) * e->n;
   double* dst[6] = {x, y, z, vx, vy, vz};
@@ -646,6 +649,7 @@ nbody_status nbody_get_derivs(nbody_engine* e, double* ax, double* ay, double* a
 }
 
 nbody_status nbody_acc_jerk(nbody_engine* e) {
+  TraceRange trace_("nbody_acc_jerk");
   NB_TRY(need_state(e));
   return eval_current(e);
 }
@@ -669,6 +673,7 @@ nbody_status nbody_correct(nbody_engine* e) {
 }
 
 nbody_status nbody_step(nbody_engine* e, int nsteps) {
+  TraceRange trace_("nbody_step");
   NB_TRY(need_state(e));
   if (nsteps < 0) return fail(NBODY_ERR_INVALID_ARG, "nsteps < 0");
   if (!e->have_derivs) NB_TRY(eval_current(e));
@@ -684,6 +689,7 @@ nbody_status nbody_synchronize(nbody_engine* e) {
 }
 
 nbody_status nbody_energy(nbody_engine* e, int ref_compat, double* T, double* U) {
+  TraceRange trace_("nbody_energy");
   NB_TRY(need_state(e));
   const int nb = e->ld / kBlockO1;
   double* scal = e->partial + nb;  // two result slots after the partials
@@ -761,6 +767,7 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
                                    const double* z, const double* m, const double* vx,
                                    const double* vy, const double* vz, double* ax, double* ay,
                                    double* az, double* jx, double* jy, double* jz, void* stream) {
+  TraceRange trace_("nbody_acc_jerk_device");
   NB_TRY(check_engine(e));
   if (n < 1 || n > e->n) return fail(NBODY_ERR_INVALID_ARG, "n = %d outside [1, %d]", n, e->n);
   const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
@@ -807,6 +814,7 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
                                                 const double* vx, const double* vy,
                                                 const double* vz, double* ax, double* ay,
                                                 double* az, double* jx, double* jy, double* jz) {
+  TraceRange trace_("nbody_force_calculation");
   if (n < 1) return fail(NBODY_ERR_INVALID_ARG, "n = %d", n);
   if (i_begin < 0 || i_end > n || i_begin > i_end)
     return fail(NBODY_ERR_INVALID_ARG, "row range [%d, %d) outside [0, %d)", i_begin, i_end, n);

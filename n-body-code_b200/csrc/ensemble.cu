@@ -31,6 +31,7 @@
 #include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
+#include "trace.h"
 
 using namespace nbody;
 
@@ -584,6 +585,7 @@ nbody_status nbody_ensemble_acc_jerk(nbody_ensemble* e) {
 }
 
 nbody_status nbody_ensemble_step(nbody_ensemble* e, int nsteps) {
+  TraceRange trace_("nbody_ensemble_step");
   EN_TRY(ens_check(e));
   if (nsteps < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "nsteps < 0");
   if (!e->have_derivs) EN_TRY(ens_eval_current(e));

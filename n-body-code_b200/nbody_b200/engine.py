@@ -120,6 +120,28 @@ class Engine:
     def synchronize(self) -> None:
         check(self._L.nbody_synchronize(self._h), "nbody_synchronize")
 
+    def cycle(self, state: dict, ncycle: int, ref_compat: bool = False) -> dict:
+        """The reference's run (NBody::cycle, src/nbody.cpp:291-380): upload
+        the bodies, first force evaluation (and initial dt when adaptive),
+        E0, ncycle steps with per-phase timers, final energy; returns the
+        reference's reported quantities (initE, finE, Q, Err and the per-cycle
+        PRED / EVAL / CORR seconds)."""
+        self.set_state(state)
+        self.force_calculation()
+        T0, U0 = self.energy(ref_compat)
+        pred, ev, corr = [], [], []
+        for _ in range(int(ncycle)):
+            self.timestepping(1)
+            t = self.timers()
+            pred.append(t["pred_ms"] * 1e-3)
+            ev.append(t["eval_ms"] * 1e-3)
+            corr.append(t["corr_ms"] * 1e-3)
+        T1, U1 = self.energy(ref_compat)
+        e0, e1 = T0 + U0, T1 + U1
+        return {"initE": e0, "finE": e1, "Q": -2.0 * T1 / U1, "Err": abs(e1 - e0) / abs(e0),
+                "t_predv": pred, "t_evalv": ev, "t_corrv": corr,
+                "t_eval_init": self.timers()["eval_init_ms"] * 1e-3}
+
     def energy(self, ref_compat: bool = False) -> tuple[float, float]:
         T, U = C.c_double(), C.c_double()
         check(self._L.nbody_energy(self._h, int(ref_compat), C.byref(T), C.byref(U)), "nbody_energy")
