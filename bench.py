@@ -450,7 +450,7 @@ def main_ensemble(a):
                                f"eps = 4/N, dt = 1/512, {a.precision}",
                    "bodies": int(sizes.sum()), "interactions_per_step": inter,
                    "l2": "inputs larger than L2 (no flush)"},
-        "ensemble": {k: info[k] for k in ("items", "tiles_per_item", "grid", "padded_rows")},
+        "ensemble": {k: info[k] for k in ("items", "tiles_per_item", "j_tile", "threads", "grid", "padded_rows")},
         "launch_per_cluster_serial": {
             "ms_per_step": serial_ms, "value": inter / (serial_ms * 1e-3) / 1e9,
             "how": "one single-system engine per cluster stepped one at a time; sum of each "

@@ -201,12 +201,13 @@ typedef struct {
   const double* dt;      /* fixed shared step per cluster (> 0)              */
   int precision;         /* nbody_precision                                  */
   int device;
-  int tiles_per_item;    /* j-tiles (128 bodies) per work item; 0 = default 8,
-                            or chosen by timing when tune = 1               */
+  int tiles_per_item;    /* j-tiles per work item; 0 = default 8, or (with the
+                            kernel shape) chosen by timing when tune = 1    */
   int tune;
 } nbody_ensemble_config;
 typedef struct {
   int nclusters, padded_rows, items, tiles_per_item, grid;
+  int threads, j_tile;           /* persistent kernel shape in use */
   double interactions_per_step;  /* sum of n[c]^2 */
   long long steps;
   double last_step_ms;           /* CUDA events around the last graph step */

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -38,13 +40,7 @@ using namespace nbody;
 namespace {
 
 constexpr int kPadRows = 256;  // cluster padding = rows per work item
-constexpr int kTile = 128;     // j-tile size of the ensemble kernels
 constexpr int kBlock = 256;
-
-using RowsEnsFP64 = RowsFP64<128, 2, kTile, 1>;              // 256 rows
-using RowsEnsMixed = RowsMixedX2<64, 4, kTile, 1, 1>;        // 256 rows
-static_assert(RowsEnsFP64::ROWS == kPadRows && RowsEnsMixed::ROWS == kPadRows,
-              "an item's row block is one padding unit");
 
 struct ClusterDev {
   int row0, n, ld, S;
@@ -210,9 +206,30 @@ __global__ void ens_energy_sum_kernel(const ClusterDev* __restrict__ cl, const d
   }
 }
 
+// Persistent-kernel shapes (all with 256-row items = one padding unit); the
+// first of each precision is the default, the autotuner times all of them.
+struct EnsKernel {
+  int precision, nt, tile;
+  const void* fn;
+  size_t smem;
+};
+
 template <class R>
-const void* ens_kernel() {
-  return reinterpret_cast<const void*>(&ensemble_pair_kernel<R>);
+EnsKernel ens_kernel(int precision) {
+  static_assert(R::ROWS == kPadRows, "an item's row block is one padding unit");
+  return {precision, R::NT, R::TJ, reinterpret_cast<const void*>(&ensemble_pair_kernel<R>),
+          pair_smem_bytes<R>()};
+}
+
+const std::vector<EnsKernel>& ens_registry() {
+  static const std::vector<EnsKernel> r = {
+      ens_kernel<RowsFP64<128, 2, 128, 1>>(NBODY_FP64),
+      ens_kernel<RowsFP64<256, 1, 128, 4>>(NBODY_FP64),
+      ens_kernel<RowsMixedX2<64, 4, 128, 1, 1>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<128, 2, 128, 1, 1>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<64, 4, 64, 1, 1>>(NBODY_MIXED),
+  };
+  return r;
 }
 
 }  // namespace
@@ -220,6 +237,7 @@ const void* ens_kernel() {
 struct nbody_ensemble {
   int C = 0, L = 0, dev = 0, sms = 0, precision = 0;
   int tiles_per_item = 8;
+  const EnsKernel* kern = nullptr;  // persistent pair kernel in use
   int grid = 0;
   long long interactions = 0;  // sum of n_c^2 per step
   cudaStream_t stream = nullptr;
@@ -265,7 +283,7 @@ nbody_status build_items(nbody_ensemble* e, int tpi) {
   std::vector<EnsItem> items;
   long long p_off = 0;
   for (int c = 0; c < e->C; ++c) {
-    const int tiles = e->ld[c] / kTile;
+    const int tiles = e->ld[c] / e->kern->tile;
     const int S = (tiles + tpi - 1) / tpi;
     cl[c] = ClusterDev{e->row0[c], e->n[c], e->ld[c], S, p_off, e->eps2[c], e->dt[c]};
     for (int rb = 0; rb < e->ld[c] / kPadRows; ++rb)
@@ -308,13 +326,23 @@ nbody_status build_items(nbody_ensemble* e, int tpi) {
 nbody_status launch_ens_pair(nbody_ensemble* e) {
   EN_CUDA(cudaMemsetAsync(e->counter, 0, sizeof(unsigned int), e->stream));
   const bool fp64 = e->precision == NBODY_FP64;
-  const void* fn = fp64 ? ens_kernel<RowsEnsFP64>() : ens_kernel<RowsEnsMixed>();
-  const size_t smem = fp64 ? pair_smem_bytes<RowsEnsFP64>() : pair_smem_bytes<RowsEnsMixed>();
-  const int nt = fp64 ? RowsEnsFP64::NT : RowsEnsMixed::NT;
   const void* jb = fp64 ? static_cast<const void*>(e->jb64) : static_cast<const void*>(e->jbx);
   void* args[] = {const_cast<void*>(static_cast<const void*>(&jb)), &e->items, &e->n_items,
                   &e->counter, &e->P, &e->status};
-  EN_CUDA(cudaLaunchKernel(fn, dim3(e->grid), dim3(nt), args, smem, e->stream));
+  EN_CUDA(cudaLaunchKernel(e->kern->fn, dim3(e->grid), dim3(e->kern->nt), args, e->kern->smem,
+                           e->stream));
+  return NBODY_OK;
+}
+
+// Selects a persistent kernel: opts in to its shared memory and sizes the
+// grid to the SMs x resident CTAs it reaches.
+nbody_status use_kernel(nbody_ensemble* e, const EnsKernel* k) {
+  EN_CUDA(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(k->smem)));
+  int occ = 0;
+  EN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k->fn, k->nt, k->smem));
+  e->kern = k;
+  e->grid = e->sms * std::max(occ, 1);
   return NBODY_OK;
 }
 
@@ -367,31 +395,43 @@ nbody_status ens_build_graph(nbody_ensemble* e) {
   return NBODY_OK;
 }
 
-// Times the pair launch for each candidate item size; keeps the fastest.
+// Times the pair launch for every (kernel shape, item size) pair; keeps the
+// fastest.  Items count j-tiles, so tiles_per_item x tile = j per item.
 nbody_status ens_autotune(nbody_ensemble* e) {
   EN_TRY(launch_ens_pack(e));
   cudaEvent_t a, b;
   EN_CUDA(cudaEventCreate(&a));
   EN_CUDA(cudaEventCreate(&b));
   float best = 1e30f;
-  int best_tpi = e->tiles_per_item;
-  for (int tpi : {2, 4, 8, 16, 32, 64}) {
-    EN_TRY(build_items(e, tpi));
-    EN_TRY(launch_ens_pair(e));
-    EN_CUDA(cudaEventRecord(a, e->stream));
-    for (int r = 0; r < 2; ++r) EN_TRY(launch_ens_pair(e));
-    EN_CUDA(cudaEventRecord(b, e->stream));
-    EN_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    EN_CUDA(cudaEventElapsedTime(&ms, a, b));
-    if (ms < best) {
-      best = ms;
-      best_tpi = tpi;
+  const EnsKernel* best_k = e->kern;
+  int best_tpi = 8;
+  for (const EnsKernel& k : ens_registry()) {
+    if (k.precision != e->precision) continue;
+    EN_TRY(use_kernel(e, &k));
+    for (int j_per_item : {256, 512, 1024, 2048, 4096, 8192}) {
+      const int tpi = std::max(1, j_per_item / k.tile);
+      EN_TRY(build_items(e, tpi));
+      EN_TRY(launch_ens_pair(e));
+      EN_CUDA(cudaEventRecord(a, e->stream));
+      for (int r = 0; r < 2; ++r) EN_TRY(launch_ens_pair(e));
+      EN_CUDA(cudaEventRecord(b, e->stream));
+      EN_CUDA(cudaEventSynchronize(b));
+      float ms = 0;
+      EN_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (getenv("NBODY_TUNE_VERBOSE"))
+        fprintf(stderr, "[nbody ens tune] nt=%d tile=%d tiles_per_item=%d  %.4f ms\n", k.nt, k.tile,
+                tpi, ms / 2);
+      if (ms < best) {
+        best = ms;
+        best_k = &k;
+        best_tpi = tpi;
+      }
     }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   EN_TRY(ens_status(e));
+  EN_TRY(use_kernel(e, best_k));
   return build_items(e, best_tpi);
 }
 
@@ -498,14 +538,11 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     EN_CUDA(cudaMalloc(&raw->Tc, sizeof(double) * raw->C));
     EN_CUDA(cudaMalloc(&raw->Uc, sizeof(double) * raw->C));
     for (auto& ev : raw->ev) EN_CUDA(cudaEventCreate(&ev));
-    const bool fp64 = raw->precision == NBODY_FP64;
-    const void* fn = fp64 ? ens_kernel<RowsEnsFP64>() : ens_kernel<RowsEnsMixed>();
-    const size_t smem = fp64 ? pair_smem_bytes<RowsEnsFP64>() : pair_smem_bytes<RowsEnsMixed>();
-    const int nt = fp64 ? RowsEnsFP64::NT : RowsEnsMixed::NT;
-    EN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    int occ = 0;
-    EN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nt, smem));
-    raw->grid = raw->sms * std::max(occ, 1);
+    for (const EnsKernel& k : ens_registry())
+      if (k.precision == raw->precision) {
+        EN_TRY(use_kernel(raw, &k));
+        break;
+      }
     return build_items(raw, cfg->tiles_per_item > 0 ? cfg->tiles_per_item : 8);
   };
   nbody_status s = body();
@@ -624,6 +661,8 @@ nbody_status nbody_ensemble_info(nbody_ensemble* e, nbody_ensemble_info_t* out) 
   out->padded_rows = e->L;
   out->items = e->n_items;
   out->tiles_per_item = e->tiles_per_item;
+  out->j_tile = e->kern->tile;
+  out->threads = e->kern->nt;
   out->grid = e->grid;
   out->interactions_per_step = static_cast<double>(e->interactions);
   out->steps = e->steps;

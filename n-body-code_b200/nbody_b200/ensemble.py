@@ -20,8 +20,8 @@ class EnsembleConfig(C.Structure):
 
 class EnsembleInfo(C.Structure):
     _fields_ = [("nclusters", C.c_int), ("padded_rows", C.c_int), ("items", C.c_int),
-                ("tiles_per_item", C.c_int), ("grid", C.c_int),
-                ("interactions_per_step", C.c_double), ("steps", C.c_longlong),
+                ("tiles_per_item", C.c_int), ("grid", C.c_int), ("threads", C.c_int),
+                ("j_tile", C.c_int), ("interactions_per_step", C.c_double), ("steps", C.c_longlong),
                 ("last_step_ms", C.c_double)]
 
 

@@ -114,4 +114,4 @@ def test_plummer_ensemble_config():
         de[prec] = np.abs((T1 + U1) - (T0 + U0)) / np.abs(T0 + U0)
     assert np.all(np.isfinite(de["mixed"]))
     assert np.all(de["mixed"] <= 2.0 * de["fp64"] + 1e-9), np.max(de["mixed"] / (de["fp64"] + 1e-12))
-    assert info["tiles_per_item"] in (2, 4, 8, 16, 32, 64)
+    assert info["tiles_per_item"] * info["j_tile"] in (256, 512, 1024, 2048, 4096, 8192)
