@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"))
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--tune", action="store_true", help="autotune pair-kernel tiling first")
+    ap.add_argument("--variant", type=int, default=0,
+                    help="mixed pair kernel (nbody_config.pair_variant): 0 = tile-relative (default), "
+                         "1 = scalar hi/lo, 2/3 = packed hi/lo")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--kernels-only", action="store_true",
@@ -136,12 +139,13 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def traffic_per_launch(precision):
-    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+def traffic_per_launch(kernel):
+    """DRAM bytes per pair-kernel launch (the headline workload) from the
+    committed ncu summary, by kernel name."""
     path = os.path.join(ROOT, "profiles", "pair_kernel_dram.json")
     try:
         with open(path) as f:
-            return json.load(f).get(precision)
+            return json.load(f).get(kernel)
     except (OSError, ValueError):
         return None
 
@@ -150,7 +154,8 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
     import nbody_b200 as nb
     n = a.n
     clk = ClockSampler(dev).__enter__()  # sampling starts before the warm-up so the timed region is covered
-    e = nb.Engine(n, eps2=a.eps ** 2, precision=precision, device=dev, dt=a.dt, tune=a.tune)
+    e = nb.Engine(n, eps2=a.eps ** 2, precision=precision, device=dev, dt=a.dt, tune=a.tune,
+                  pair_variant=a.variant if precision == "mixed" else 0)
     e.set_state(state)
     e.force_calculation()
     T0, U0 = e.energy()
@@ -158,6 +163,7 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{dev}")
     e.timestepping(a.warmup)
     e.synchronize()
+    reorders0 = e.timers()["reorders"]
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     pair_ms, pred_ms, corr_ms = [], [], []
@@ -179,6 +185,9 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
         dist.barrier()
     step_ms = [s.elapsed_time(t) for s, t in zip(starts, ends)]
     tm = e.timers()
+    # kernels of the timed steps: the captured step graph each step, plus the
+    # captured Morton re-ordering where one ran (tile-relative kernel)
+    launches = tm["step_kernels"] * a.steps + tm["order_kernels"] * (tm["reorders"] - reorders0)
     if a.time_units > 0:  # carry on (untimed) to the requested model time
         rest = int(round(a.time_units / a.dt)) - a.warmup - a.steps
         while rest > 0:
@@ -200,7 +209,8 @@ def run_arm(a, precision, state, torch, dist, rank, world, dev):
         "E0": T0 + U0,
         "tiling": {k: tm[k] for k in ("threads", "i_per_thread", "j_tile", "split_j")},
         "clocks": clk.summary(),
-        "launches": 3 * a.steps,
+        "launches": int(launches),
+        "record_format": tm["record_format"],
     }
 
 
@@ -415,7 +425,10 @@ def main_ensemble(a):
     engines = []
     off = np.concatenate([[0], np.cumsum(sizes)])
     for c, n in enumerate(sizes):
-        e = nb.Engine(int(n), eps2=float(eps2[c]), precision=a.precision, dt=dt)
+        # the single-system engines run the ensemble kernel's pair arithmetic
+        # (packed hi/lo for mixed)
+        e = nb.Engine(int(n), eps2=float(eps2[c]), precision=a.precision, dt=dt,
+                      pair_variant=3 if a.precision == "mixed" else 0)
         e.set_state({k: state[k][off[c]:off[c + 1]] for k in nb.FIELDS})
         e.force_calculation()
         e.timestepping(1)
@@ -552,7 +565,8 @@ def main():
     if a.accuracy and rank == 0:
         d = {}
         for prec in ("fp64", "mixed"):
-            with nb.Engine(a.n, eps2=a.eps ** 2, precision=prec, device=dev, dt=a.dt) as e:
+            with nb.Engine(a.n, eps2=a.eps ** 2, precision=prec, device=dev, dt=a.dt,
+                           pair_variant=a.variant if prec == "mixed" else 0) as e:
                 e.set_state(state)
                 e.force_calculation()
                 d[prec] = e.get_derivs()
@@ -578,12 +592,16 @@ def main():
     inter = float(a.n) * a.n
     value = replica_value(world, inter, ms)
 
+    kernel_names = {0: "pair_fp64_kernel", 1: "pair_mixed_kernel", 2: "pair_mixed_x2_kernel",
+                    3: "pair_mixed_rel_kernel"}
+
     def roofline(arm, prec):
         peak = peaks["fp32_tflops"] if prec == "mixed" else peaks["fp64_tflops"]
         achieved = FLOP_PER_INTERACTION * inter / (arm["pair_ms"] * 1e-3) / 1e12
         return {"bound": "fp32" if prec == "mixed" else "fp64", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic_per_launch(prec),
-                "kernel": f"pair_{'mixed' if prec == 'mixed' else 'fp64'}_kernel",
+                "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic_per_launch(kernel_names[arm["record_format"]]),
+                "kernel": kernel_names[arm["record_format"]],
                 "peak_source": "measured live by nbody_measure_peaks (FMA microkernel, this GPU)",
                 "flop_per_interaction": FLOP_PER_INTERACTION}
 

@@ -65,10 +65,16 @@ typedef struct {
   double eta0;        /* initial-dt criterion, default 1e-4 (nbody.h:15)    */
   int tune;           /* 1: time candidate tilings on first use (autotuner) */
   int threads, i_per_thread, j_tile, split_j; /* 0 = choose automatically   */
-  int pair_variant;   /* mixed only: 0 = packed-pair (f32x2) kernel with
-                         FP64 accumulators in shared memory, 1 = scalar
-                         FP32 kernel, 2 = packed-pair kernel with FP64
-                         accumulators in registers                          */
+  int pair_variant;   /* mixed only: 0 = packed-pair (f32x2) kernel on
+                         tile-relative positions (Morton-ordered j-tiles,
+                         one add per separation component; the fastest),
+                         1 = scalar FP32 kernel on hi/lo positions,
+                         2 = packed-pair hi/lo kernel, FP64 accumulators in
+                         registers, 3 = packed-pair hi/lo kernel, FP64
+                         accumulators in shared memory (the most accurate) */
+  int sort_every;     /* variant 0: re-order the j-bodies along the Morton
+                         curve every this many steps (tile centres and
+                         offsets are rebuilt every step); 0 = 16          */
 } nbody_config;
 
 typedef struct nbody_engine nbody_engine;
@@ -82,6 +88,12 @@ typedef struct {
   int threads, i_per_thread, j_tile, split_j; /* tiling in use          */
   long long steps;                  /* Hermite steps taken                  */
   double t, dt;                     /* model time and current shared dt     */
+  int record_format;                /* j-records of the pair kernel in use:
+                                       0 FP64, 1 FP32 hi/lo, 2 packed hi/lo,
+                                       3 packed tile-relative (Morton tiles) */
+  int step_kernels;                 /* kernel launches in one captured step */
+  long long reorders;               /* Morton re-orderings run by steps     */
+  int order_kernels;                /* kernel launches in one re-ordering   */
 } nbody_timers;
 
 /* Fill *cfg with defaults: eps2 = 1e-7, FP64, device 0, adaptive dt,
@@ -170,8 +182,8 @@ nbody_status nbody_acc_jerk_device(nbody_engine* eng, int n, const double* x, co
  * device memory (an application that owns the device memory budget through
  * its own pool, a real-time loop where cudaMalloc/cudaFree would stall the
  * device, code running inside someone else's time-step loop): same inputs,
- * outputs and physics as nbody_acc_jerk_device, but no engine and no
- * cudaMalloc - its scratch is a 16 MiB static device array inside the
+ * outputs and physics as nbody_acc_jerk_device (mixed precision: the packed
+ * hi/lo kernel, pair_variant 3), but no engine and no cudaMalloc - its scratch is a 16 MiB static device array inside the
  * library, held by every GPU that loads the library until the process exits.
  * n must be <= 32768 (NBODY_ERR_INVALID_ARG beyond).  Arrays are float64 on
  * the current device; work is enqueued on `stream` (cudaStream_t, NULL = the

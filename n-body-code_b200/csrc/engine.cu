@@ -5,14 +5,22 @@
 //   state  [13][ld] float64  X(3) V(3) M(1) D(6)  (D = current acc, jerk)
 //   P      [S][6][ld]        split-j partial sums of the pair kernel
 //   jb64   [ld] JBody64      FP64 j-records (also used by the potential)
-//   jb32   [ld] JBody32      mixed-precision j-records (mixed engines)
+//   jb32   [ld] JBody32      mixed-precision j-records (mixed engines):
+//                            JBody32, JBodyX2, or tiles of JBodyRel
+//   sort   keys, indices, order, CUB scratch of the Morton ordering that
+//          builds the JBodyRel tiles (mixed engines)
 //   ctl    StepCtl           dt, t, Aarseth criterion, step counter
 // ld = n rounded up to a multiple of 256 (kPad).
 //
-// A Hermite step is three launches - predict (O(N), writes the j-records),
-// pair (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
-// correction + dt criterion) - captured once into a CUDA graph and replayed.
+// A Hermite step - predict (O(N), writes the j-records; the tile-relative
+// mixed kernel's records come from rel_tile_kernel right after), pair
+// (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
+// correction + dt criterion) - is captured once into a CUDA graph and
+// replayed.  The Morton re-ordering of the tile-relative records is a
+// second captured graph, replayed ahead of every sort_every-th step.
 #include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -32,6 +40,7 @@
 #include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
+#include "reltiles.cuh"
 #include "trace.h"
 
 using namespace nbody;
@@ -41,6 +50,7 @@ namespace {
 constexpr int kPad = 256;        // body padding granularity (multiple of every j-tile)
 constexpr int kMaxSplit = 64;    // split-j upper bound
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
+constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
 
 thread_local std::string g_last_error;
 
@@ -97,6 +107,14 @@ PairKernel make_mixed_x2() {
           2 * TJ * sizeof(JBodyX2) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU, MINB};
 }
 
+template <int NT, int IPT, int TJ, int ACC = 1, int JU = 1, int MINB = 1>
+PairKernel make_mixed_rel() {
+  return {NBODY_MIXED, NT, IPT, TJ, kRecRel,
+          reinterpret_cast<const void*>(&pair_mixed_rel_kernel<NT, IPT, TJ, ACC, JU, MINB>),
+          2 * (TJ + 1) * sizeof(JBodyRel) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU,
+          MINB};
+}
+
 // The first entry of each shape/variant is the one explicit tilings select;
 // the autotuner times all of them.
 const std::vector<PairKernel>& registry() {
@@ -105,6 +123,10 @@ const std::vector<PairKernel>& registry() {
       make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
       make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
       make_fp64<128, 2, 128, 1, 6>(), make_fp64<128, 2, 64, 1, 6>(), make_fp64<128, 1, 128, 4, 8>(),
+      // tile-relative packed pairs (Morton-ordered j-tiles; default mixed)
+      make_mixed_rel<128, 4, 128>(), make_mixed_rel<64, 4, 128>(),  make_mixed_rel<128, 2, 128>(),
+      make_mixed_rel<256, 2, 128>(), make_mixed_rel<256, 4, 128>(), make_mixed_rel<128, 2, 64>(),
+      make_mixed_rel<128, 4, 64>(),  make_mixed_rel<128, 2, 256>(), make_mixed_rel<128, 4, 128, 0, 2>(),
       // packed pairs, FP64 accumulators in shared memory (default)
       make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
       make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
@@ -122,9 +144,10 @@ const std::vector<PairKernel>& registry() {
   return r;
 }
 
-// variant (mixed only): 0 = packed pairs with shared-memory FP64
-// accumulators (falling back to register accumulators where that shape has
-// none), 1 = scalar FP32, 2 = packed pairs with register accumulators.
+// variant (mixed only): 0 = tile-relative packed pairs, 1 = scalar FP32
+// hi/lo, 2 = packed hi/lo pairs with register accumulators, 3 = packed
+// hi/lo pairs with shared-memory FP64 accumulators (falling back to
+// register accumulators where that shape has none).
 const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
   auto match = [&](int fmt, int acc) -> const PairKernel* {
     for (const auto& k : registry())
@@ -135,10 +158,14 @@ const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int varian
   };
   if (precision == NBODY_FP64) return match(kRecF64, -1);
   if (variant == 1) return match(kRecF32, -1);
+  if (variant == 0) return match(kRecRel, -1);
   if (variant == 2) return match(kRecX2, 0);
   const PairKernel* k = match(kRecX2, 1);
   return k ? k : match(kRecX2, 0);
 }
+
+// Record format of a precision's variant-0 kernels (the autotuner's family).
+int default_format(int precision) { return precision == NBODY_FP64 ? kRecF64 : kRecRel; }
 
 struct Tiling {
   const PairKernel* k = nullptr;
@@ -173,12 +200,24 @@ struct nbody_engine {
   JBody64* jb64 = nullptr;
   void* jb32 = nullptr;  // mixed records: JBody32 or JBodyX2 (sized for the larger)
   JBody64* jbe = nullptr;  // records of the energy diagnostic (never a pair kernel's input)
+  // Morton ordering of the tile-relative records (mixed engines)
+  uint64_t* sort_keys = nullptr;  // [2][ld]: keys, sorted keys
+  int* sort_idx = nullptr;        // [2][ld]: indices, sorted indices (= order)
+  double* bbox_part = nullptr;    // [kMaxBBoxParts][6]
+  void* sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+  bool order_own = false;         // the order is of this engine's own n bodies
+  int since_sort = 0;             // steps since that order was made
   StepCtl* ctl = nullptr;
   double* partial = nullptr;  // reduction scratch: ld / 256 + 1 doubles + 4 scalars
   int* status = nullptr;
   Tiling tiling;
   bool tiled = false;
   cudaGraphExec_t graph = nullptr;
+  int graph_kernels = 0;  // kernel nodes of the captured step
+  cudaGraphExec_t order_graph = nullptr;  // captured Morton re-ordering (variant 0)
+  int order_kernels = 0;
+  long long reorders = 0;  // re-orderings run before steps
   bool have_state = false, have_derivs = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_init[2] = {nullptr, nullptr};
@@ -261,14 +300,23 @@ nbody_status prepare_kernel(const PairKernel& k) {
   return NBODY_OK;
 }
 
+SoA7 own_inputs(nbody_engine* e);
+
+// src / n_src: the inputs the records were built from (the tile-relative
+// kernel reads its i-rows there); nullptr = the engine's own state.
 nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_end,
-                         cudaStream_t st) {
+                         cudaStream_t st, const SoA7* src = nullptr, int n_src = 0) {
   const PairKernel& k = *t.k;
   NB_TRY(prepare_kernel(k));
   PairArgs a;
   a.i_begin = i_begin;
   a.i_end = i_end;
   a.n_rows_pad = e->ld;
+  if (k.fmt == kRecRel) {
+    const SoA7 in = src ? *src : own_inputs(e);
+    a.rows = RowSrc{in.x, in.y, in.z, in.vx, in.vy, in.vz};
+    a.n_rows_pad = src ? n_src : e->n;
+  }
   a.n_tiles = e->ld / k.tj;
   a.tiles_per_split = (a.n_tiles + t.split - 1) / t.split;
   a.eps2 = e->cfg.eps2;
@@ -285,8 +333,8 @@ nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_en
   return NBODY_OK;
 }
 
-SoA7 own_inputs(nbody_engine* e);
-nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt);
+nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
+                         int tj);
 
 nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   const auto key = std::make_tuple(e->dev, e->cfg.precision, e->ld, rows);
@@ -307,9 +355,9 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   const auto& reg = registry();
   for (size_t idx = 0; idx < reg.size(); ++idx) {
     const PairKernel& k = reg[idx];
-    if (k.precision != e->cfg.precision) continue;
+    if (k.precision != e->cfg.precision || k.fmt != default_format(k.precision)) continue;
     const int s0 = choose_split(e, k, rows);
-    NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt));
+    NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt, k.tj));
     for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
       NB_TRY(ensure_partials(e, s));
       Tiling t{&k, s};
@@ -344,8 +392,10 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
 // Tiling for `rows` i-rows: explicit config, else tuned, else heuristic.
 nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
   const nbody_config& c = e->cfg;
+  // defaults: the best measured shape of each family (Plummer N = 65536)
+  const bool rel = c.precision == NBODY_MIXED && c.pair_variant == 0;
   int nt = c.threads ? c.threads : 128;
-  int ipt = c.i_per_thread ? c.i_per_thread : 2;
+  int ipt = c.i_per_thread ? c.i_per_thread : (rel ? 4 : 2);
   int tj = c.j_tile ? c.j_tile : 128;
   const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, c.pair_variant);
   if (!k)
@@ -376,22 +426,83 @@ SoA6 own_derivs(nbody_engine* e) {
   return SoA6{D, D + ld, D + 2 * ld, D + 3 * ld, D + 4 * ld, D + 5 * ld};
 }
 
-// Writes the FP64 records (always: the potential reads them) and, for a
-// mixed kernel, the records in that kernel's format.
-nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt) {
-  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      n, e->ld, in, e->jb64, fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
-      fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
+// Morton order of bodies [0, n) of `in` (bounding box, keys, stable sort)
+// into sort_idx + ld; own = the inputs are the engine's state.
+nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st,
+                                  bool own) {
+  const int parts = std::min(kMaxBBoxParts, (n + kBBoxThreads - 1) / kBBoxThreads);
+  bbox_partial_kernel<<<parts, kBBoxThreads, 0, st>>>(n, in, e->bbox_part);
+  NB_CUDA(cudaGetLastError());
+  const size_t ld = e->ld;
+  morton_key_kernel<<<(n + kBBoxThreads - 1) / kBBoxThreads, kBBoxThreads, 0, st>>>(
+      n, in, e->bbox_part, parts, e->sort_keys, e->sort_idx);
+  NB_CUDA(cudaGetLastError());
+  size_t bytes = e->sort_tmp_bytes;
+  NB_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + ld,
+                                          e->sort_idx, e->sort_idx + ld, n, 0, 63, st));
+  e->order_own = own && n == e->n;
+  e->since_sort = 0;
+  return NBODY_OK;
+}
+
+// Tiles of tj tile-relative records of bodies [0, n) of `in`, in the order
+// of the last enqueue_morton_order.
+nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int tj) {
+  const int* order = e->sort_idx + e->ld;
+  JBodyRel* out = static_cast<JBodyRel*>(e->jb32);
+  const int tiles = e->ld / tj;
+  switch (tj) {
+    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(n, in, order, out); break;
+    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(n, in, order, out); break;
+    case 256: rel_tile_kernel<256><<<tiles, 256, 0, st>>>(n, in, order, out); break;
+    default: return fail(NBODY_ERR_INVALID_ARG, "no tile-relative record builder for j_tile %d", tj);
+  }
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
 
+// Writes the FP64 records (always: the potential reads them) and, for a
+// mixed kernel, the records in that kernel's format (tiles of tj bodies;
+// tile-relative records are re-ordered first).
+nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
+                         int tj) {
+  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      n, e->ld, in, e->jb64, fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
+      fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
+  NB_CUDA(cudaGetLastError());
+  if (fmt == kRecRel) {
+    NB_TRY(enqueue_morton_order(e, n, in, st, in.x == e->X));
+    NB_TRY(build_rel_tiles(e, n, in, st, tj));
+  }
+  return NBODY_OK;
+}
+
 int tiling_fmt(const nbody_engine* e) { return e->tiled ? e->tiling.k->fmt : kRecF64; }
+int tiling_tj(const nbody_engine* e) { return e->tiled ? e->tiling.k->tj : 0; }
+int sort_period(const nbody_engine* e) { return e->cfg.sort_every > 0 ? e->cfg.sort_every : 16; }
+
+// Before a step of the engine's own state: re-order when the order is stale
+// (another system's, or sort_every steps old).
+nbody_status maybe_reorder(nbody_engine* e, cudaStream_t st) {
+  if (tiling_fmt(e) != kRecRel) return NBODY_OK;
+  if (!e->order_own || e->since_sort >= sort_period(e)) {
+    if (e->order_graph && st == e->stream) {
+      NB_CUDA(cudaGraphLaunch(e->order_graph, st));
+      e->order_own = true;
+      e->since_sort = 0;
+    } else {
+      NB_TRY(enqueue_morton_order(e, e->n, own_inputs(e), st, true));
+    }
+    ++e->reorders;
+  }
+  ++e->since_sort;
+  return NBODY_OK;
+}
 
 // acc + jerk of the engine's current X, V, M into D (rows [0, n)).
 nbody_status eval_current(nbody_engine* e) {
   NB_TRY(ensure_tiling(e));
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e)));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   if (!e->init_events) {
     NB_CUDA(cudaEventCreate(&e->ev_init[0]));
     NB_CUDA(cudaEventCreate(&e->ev_init[1]));
@@ -419,6 +530,7 @@ nbody_status enqueue_predict(nbody_engine* e, cudaStream_t st) {
       fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
       fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
   NB_CUDA(cudaGetLastError());
+  if (fmt == kRecRel) NB_TRY(build_rel_tiles(e, e->n, own_inputs(e), st, tiling_tj(e)));
   return NBODY_OK;
 }
 
@@ -427,6 +539,21 @@ nbody_status enqueue_correct(nbody_engine* e, cudaStream_t st) {
       e->n, e->ld, e->tiling.split, e->P, e->X, e->V, e->D, e->ctl, e->cfg.eta);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
+}
+
+int count_kernel_nodes(cudaGraph_t g) {
+  size_t nodes = 0;
+  int kernels = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+    std::vector<cudaGraphNode_t> v(nodes);
+    if (cudaGraphGetNodes(g, v.data(), &nodes) == cudaSuccess)
+      for (size_t k = 0; k < nodes; ++k) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(v[k], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel)
+          ++kernels;
+      }
+  }
+  return kernels;
 }
 
 nbody_status build_step_graph(nbody_engine* e) {
@@ -456,11 +583,36 @@ nbody_status build_step_graph(nbody_engine* e) {
     return s;
   }
   if (ce != cudaSuccess) return fail(NBODY_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+  e->graph_kernels = count_kernel_nodes(g);
   ce = cudaGraphInstantiate(&e->graph, g, 0);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) {
     e->graph = nullptr;
     return fail(NBODY_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+  }
+  if (tiling_fmt(e) == kRecRel && !e->order_graph) {
+    // the Morton re-ordering of the engine's own state, replayed every
+    // sort_every steps ahead of the step graph
+    const bool own = e->order_own;
+    const int since = e->since_sort;
+    NB_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    s = enqueue_morton_order(e, e->n, own_inputs(e), e->stream, true);
+    g = nullptr;
+    ce = cudaStreamEndCapture(e->stream, &g);
+    e->order_own = own;  // capturing ran nothing
+    e->since_sort = since;
+    if (s != NBODY_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    if (ce != cudaSuccess) return fail(NBODY_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    e->order_kernels = count_kernel_nodes(g);
+    ce = cudaGraphInstantiate(&e->order_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      e->order_graph = nullptr;
+      return fail(NBODY_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+    }
   }
   return NBODY_OK;
 }
@@ -524,8 +676,9 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
   if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
-  if (cfg->pair_variant < 0 || cfg->pair_variant > 2)
+  if (cfg->pair_variant < 0 || cfg->pair_variant > 3)
     return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
+  if (cfg->sort_every < 0) return fail(NBODY_ERR_INVALID_ARG, "sort_every = %d", cfg->sort_every);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(NBODY_ERR_NO_DEVICE, "no CUDA device visible");
@@ -559,7 +712,17 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
     e->D = e->state + 7 * ld;
     NB_CUDA(cudaMalloc(&e->jb64, sizeof(JBody64) * ld));
     NB_CUDA(cudaMalloc(&e->jbe, sizeof(JBody64) * ld));
-    if (cfg->precision == NBODY_MIXED) NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyX2) * ld));
+    if (cfg->precision == NBODY_MIXED) {
+      static_assert(sizeof(JBodyX2) >= sizeof(JBodyRel) * 65 / 64, "jb32 holds tiles of >= 64");
+      NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyX2) * ld));
+      NB_CUDA(cudaMalloc(&e->sort_keys, sizeof(uint64_t) * 2 * ld));
+      NB_CUDA(cudaMalloc(&e->sort_idx, sizeof(int) * 2 * ld));
+      NB_CUDA(cudaMalloc(&e->bbox_part, sizeof(double) * 6 * kMaxBBoxParts));
+      NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, e->sort_tmp_bytes, e->sort_keys,
+                                              e->sort_keys + ld, e->sort_idx, e->sort_idx + ld,
+                                              static_cast<int>(ld), 0, 63, e->stream));
+      NB_CUDA(cudaMalloc(&e->sort_tmp, std::max<size_t>(e->sort_tmp_bytes, 16)));
+    }
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
     NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 + 8)));
     NB_CUDA(cudaMalloc(&e->status, sizeof(int)));
@@ -577,6 +740,7 @@ nbody_status nbody_destroy(nbody_engine* e) {
   cudaSetDevice(e->dev);
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->order_graph) cudaGraphExecDestroy(e->order_graph);
   for (auto ev : e->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto ev : e->ev_init)
@@ -586,6 +750,10 @@ nbody_status nbody_destroy(nbody_engine* e) {
   cudaFree(e->jb64);
   cudaFree(e->jb32);
   cudaFree(e->jbe);
+  cudaFree(e->sort_keys);
+  cudaFree(e->sort_idx);
+  cudaFree(e->bbox_part);
+  cudaFree(e->sort_tmp);
   cudaFree(e->ctl);
   cudaFree(e->partial);
   cudaFree(e->status);
@@ -616,7 +784,7 @@ nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, 
   c.steps = 0;
   NB_CUDA(cudaMemcpyAsync(e->ctl, &c, sizeof c, cudaMemcpyHostToDevice, e->stream));
   NB_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * ld, e->stream));
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e)));
+  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   NB_CUDA(cudaStreamSynchronize(e->stream));
   e->have_state = true;
   e->have_derivs = false;
@@ -657,6 +825,8 @@ nbody_status nbody_acc_jerk(nbody_engine* e) {
 nbody_status nbody_predict(nbody_engine* e) {
   NB_TRY(need_state(e));
   if (!e->have_derivs) NB_TRY(eval_current(e));
+  NB_TRY(ensure_tiling(e));
+  NB_TRY(maybe_reorder(e, e->stream));
   return enqueue_predict(e, e->stream);
 }
 
@@ -678,7 +848,10 @@ nbody_status nbody_step(nbody_engine* e, int nsteps) {
   if (nsteps < 0) return fail(NBODY_ERR_INVALID_ARG, "nsteps < 0");
   if (!e->have_derivs) NB_TRY(eval_current(e));
   NB_TRY(build_step_graph(e));
-  for (int k = 0; k < nsteps; ++k) NB_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    NB_TRY(maybe_reorder(e, e->stream));
+    NB_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  }
   return NBODY_OK;
 }
 
@@ -733,7 +906,11 @@ nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
     out->i_per_thread = e->tiling.k->ipt;
     out->j_tile = e->tiling.k->tj;
     out->split_j = e->tiling.split;
+    out->record_format = e->tiling.k->fmt;
   }
+  out->step_kernels = e->graph_kernels;
+  out->reorders = e->reorders;
+  out->order_kernels = e->order_kernels;
   if (e->have_state) {
     StepCtl c;
     NB_CUDA(cudaMemcpy(&c, e->ctl, sizeof c, cudaMemcpyDeviceToHost));
@@ -777,8 +954,9 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   Tiling t;
   NB_TRY(get_tiling(e, n, &t));
   NB_TRY(ensure_partials(e, t.split));
-  NB_TRY(launch_pack(e, n, SoA7{x, y, z, m, vx, vy, vz}, st, t.k->fmt));
-  NB_TRY(launch_pair(e, t, 0, n, st));
+  const SoA7 in{x, y, z, m, vx, vy, vz};
+  NB_TRY(launch_pack(e, n, in, st, t.k->fmt, t.k->tj));
+  NB_TRY(launch_pair(e, t, 0, n, st, &in, n));
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
       0, n, e->ld, t.split, e->P, SoA6{ax, ay, az, jx, jy, jz});
   NB_CUDA(cudaGetLastError());
@@ -848,7 +1026,7 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   Tiling t = e->tiling;
   if (i_end - i_begin != n) NB_TRY(get_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
-  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt));
+  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt, t.k->tj));
   NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
   if (i_end > i_begin) {
     reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(

@@ -121,7 +121,7 @@ __device__ __forceinline__ JBodyX2 make_jbx2(double x, double y, double z, doubl
 }
 
 // j-record formats of the pair kernels.
-enum RecordFormat { kRecF64 = 0, kRecF32 = 1, kRecX2 = 2 };
+enum RecordFormat { kRecF64 = 0, kRecF32 = 1, kRecX2 = 2, kRecRel = 3 };
 
 // Seven SoA input arrays (caller's or the engine's own).
 struct SoA7 {

@@ -29,6 +29,9 @@
 //          accuracy however close two bodies are), velocities and the rest
 //          of the pair math in float with the MUFU rsqrt, float partial sums
 //          over one j-tile flushed into double accumulators after each tile.
+//   Mixed, tile-relative (default): the same pair math on separations formed
+//          from per-tile float offsets (RowsMixedRel below): one add per
+//          component instead of three.
 #pragma once
 #include <cstdint>
 
@@ -55,6 +58,21 @@ struct __align__(16) JBodyX2 {
   float2 xh, yh, zh, m;
   float2 xl, yl, zl, vx;
   float2 vy, vz, pad0, pad1;
+};
+
+// j-record, tile-relative packed mixed path: 64 bytes, every field twice.
+// A j-tile's first record is a header whose x, y, z hold the tile centre c
+// (m = 0); each body record holds -D(x) with D(x) = fl(fl(c - x_hi) - x_lo),
+// x_hi = fl(x), x_lo = fl(x - x_hi).  Tiles are built from bodies in Morton
+// order, so the offsets within a tile are small.
+struct __align__(16) JBodyRel {
+  float2 x, y, z, m;
+  float2 vx, vy, vz, pad;
+};
+
+// FP64 source of the i-rows of the tile-relative kernel (body order).
+struct RowSrc {
+  const double *x, *y, *z, *vx, *vy, *vz;
 };
 
 // Packed single precision (sm_100+): one instruction performs the operation
@@ -357,6 +375,10 @@ struct RowsMixedX2 {
       xl[p] = f2_pack(b0.xl.x, b1.xl.x); yl[p] = f2_pack(b0.yl.x, b1.yl.x); zl[p] = f2_pack(b0.zl.x, b1.zl.x);
       ui[p] = f2_pack(b0.vx.x, b1.vx.x); vi[p] = f2_pack(b0.vy.x, b1.vy.x); wi[p] = f2_pack(b0.vz.x, b1.vz.x);
     }
+    init_acc(e2, extra);
+  }
+
+  __device__ __forceinline__ void init_acc(double e2, unsigned char* extra) {
 #pragma unroll
     for (int k = 0; k < NACC; ++k) {
       ax[k] = ay[k] = az[k] = 0.0;
@@ -447,6 +469,95 @@ struct RowsMixedX2 {
   }
 };
 
+// Tile-relative rows.  With c the tile centre and D(x) = fl(fl(c - x_hi) -
+// x_lo), r_ij = D(x_i) - D(x_j): the record holds -D(x_j), the row forms
+// D(x_i) once per tile.  A pair then costs one add per component instead of
+// the three of the hi/lo form (25 instead of 31 FP32 lane-ops).  The self
+// pair cancels exactly; otherwise the error of r_ij is about one float ulp
+// of |x_i - c| + |x_j - c|: for the close pairs that dominate a body's
+// force both offsets are of the order of the tile's radius, which Morton
+// ordering keeps near the local interparticle spacing.
+template <int NT_, int IPT, int TJ_, int ACC_SMEM, int JU>
+struct RowsMixedRel : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
+  using Base = RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU>;
+  using JB = JBodyRel;
+  static constexpr int NP = Base::NP, NT = NT_, TJ = TJ_;
+
+  // Rows row, row + NT, ... read (clamped to row_max) from the FP64 source.
+  __device__ __forceinline__ void begin_rows(const RowSrc& src, int row, int row_max, double e2,
+                                             unsigned char* extra) {
+    auto hl = [](double v, float& h, float& l) {
+      h = static_cast<float>(v);
+      l = static_cast<float>(v - static_cast<double>(h));
+    };
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int i0 = min(row + (2 * p) * NT, row_max), i1 = min(row + (2 * p + 1) * NT, row_max);
+      float h0, l0, h1, l1;
+      hl(src.x[i0], h0, l0); hl(src.x[i1], h1, l1);
+      this->xh[p] = f2_pack(h0, h1); this->xl[p] = f2_pack(l0, l1);
+      hl(src.y[i0], h0, l0); hl(src.y[i1], h1, l1);
+      this->yh[p] = f2_pack(h0, h1); this->yl[p] = f2_pack(l0, l1);
+      hl(src.z[i0], h0, l0); hl(src.z[i1], h1, l1);
+      this->zh[p] = f2_pack(h0, h1); this->zl[p] = f2_pack(l0, l1);
+      this->ui[p] = f2_pack(static_cast<float>(src.vx[i0]), static_cast<float>(src.vx[i1]));
+      this->vi[p] = f2_pack(static_cast<float>(src.vy[i0]), static_cast<float>(src.vy[i1]));
+      this->wi[p] = f2_pack(static_cast<float>(src.vz[i0]), static_cast<float>(src.vz[i1]));
+    }
+    this->init_acc(e2, extra);
+  }
+
+  __device__ __forceinline__ void consume(const JB* tile) {
+    const ulonglong2* hd = reinterpret_cast<const ulonglong2*>(tile);
+    const ulonglong2 c0 = hd[0], c1 = hd[1];  // (cx, cy), (cz, 0)
+    uint64_t ox[NP], oy[NP], oz[NP];           // D(x_i)
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      ox[p] = f2_sub(f2_sub(c0.x, this->xh[p]), this->xl[p]);
+      oy[p] = f2_sub(f2_sub(c0.y, this->yh[p]), this->yl[p]);
+      oz[p] = f2_sub(f2_sub(c1.x, this->zh[p]), this->zl[p]);
+    }
+    uint64_t fax[NP], fay[NP], faz[NP], fjx[NP], fjy[NP], fjz[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) fax[p] = fay[p] = faz[p] = fjx[p] = fjy[p] = fjz[p] = 0ull;
+    const uint64_t eps2 = this->eps2, m3 = this->m3;
+#pragma unroll JU
+    for (int j = 1; j <= TJ; ++j) {
+      const ulonglong2* r = reinterpret_cast<const ulonglong2*>(tile + j);
+      const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+      // r0 = (-Dx, -Dy) r1 = (-Dz, m) r2 = (vx, vy) r3 = (vz, pad)
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const uint64_t dx = f2_add(r0.x, ox[p]);
+        const uint64_t dy = f2_add(r0.y, oy[p]);
+        const uint64_t dz = f2_add(r1.x, oz[p]);
+        const uint64_t du = f2_sub(r2.x, this->ui[p]);
+        const uint64_t dv = f2_sub(r2.y, this->vi[p]);
+        const uint64_t dw = f2_sub(r3.x, this->wi[p]);
+        const uint64_t s = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, eps2)));
+        const uint64_t rv = f2_fma(dx, du, f2_fma(dy, dv, f2_mul(dz, dw)));
+        float s0, s1;
+        f2_unpack(s, s0, s1);
+        const uint64_t y = f2_pack(rsqrt_mufu(s0), rsqrt_mufu(s1));
+        const uint64_t y2 = f2_pack(rcp_mufu(s0), rcp_mufu(s1));
+        const uint64_t q = f2_mul(r1.y, f2_mul(y, y2));
+        const uint64_t c = f2_mul(rv, f2_mul(y2, m3));
+        fax[p] = f2_fma(q, dx, fax[p]);
+        fay[p] = f2_fma(q, dy, fay[p]);
+        faz[p] = f2_fma(q, dz, faz[p]);
+        fjx[p] = f2_fma(q, f2_fma(c, dx, du), fjx[p]);
+        fjy[p] = f2_fma(q, f2_fma(c, dy, dv), fjy[p]);
+        fjz[p] = f2_fma(q, f2_fma(c, dz, dw), fjz[p]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      this->flush(0, p, fax[p]); this->flush(1, p, fay[p]); this->flush(2, p, faz[p]);
+      this->flush(3, p, fjx[p]); this->flush(4, p, fjy[p]); this->flush(5, p, fjz[p]);
+    }
+  }
+};
+
 // Dynamic shared memory of a row-block kernel: two tile buffers + extras.
 template <class R>
 constexpr size_t pair_smem_bytes() {
@@ -465,6 +576,7 @@ struct PairArgs {
   double* out;             // split s, field c, row i at out[(s*6 + c)*stride + i]
   size_t stride;
   int* status;
+  RowSrc rows;             // i-row source of the tile-relative kernel (else unused)
 };
 
 template <class R>
@@ -509,6 +621,28 @@ __global__ void __launch_bounds__(NT, MINB) pair_mixed_x2_kernel(const JBodyX2* 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[2];
   pair_system<RowsMixedX2<NT, IPT, TJ, ACC_SMEM, JU>>(jb, a, smem_raw, full);
+}
+
+// Tile-relative mixed kernel: tile t is TJ + 1 records at jt + t*(TJ + 1)
+// (header first); i-rows come from a.rows, clamped below a.n_rows_pad.
+template <int NT, int IPT, int TJ, int ACC_SMEM = 1, int JU = 1, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) pair_mixed_rel_kernel(const JBodyRel* __restrict__ jt,
+                                                                  PairArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t full[2];
+  using R = RowsMixedRel<NT, IPT, TJ, ACC_SMEM, JU>;
+  constexpr int kRecs = TJ + 1;
+  TilePipe<JBodyRel, kRecs> pipe;
+  pipe.init(reinterpret_cast<JBodyRel*>(smem_raw), full);
+  const int row = a.i_begin + blockIdx.x * R::ROWS + threadIdx.x;
+  const int t_begin = blockIdx.y * a.tiles_per_split;
+  const int nt = max(0, min(a.tiles_per_split, a.n_tiles - t_begin));
+  R r;
+  r.begin_rows(a.rows, row, a.n_rows_pad - 1, a.eps2, smem_raw + 2 * kRecs * sizeof(JBodyRel));
+  if (!pipe.run(jt + static_cast<size_t>(t_begin) * kRecs, nt, a.status,
+                [&](const JBodyRel* tile) { r.consume(tile); }))
+    return;
+  r.store(a.out + static_cast<size_t>(blockIdx.y) * 6 * a.stride, a.stride, row, a.i_end);
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,7 @@ class NBodyConfig(C.Structure):
         ("j_tile", C.c_int),
         ("split_j", C.c_int),
         ("pair_variant", C.c_int),
+        ("sort_every", C.c_int),
     ]
 
 
@@ -63,6 +64,10 @@ class NBodyTimers(C.Structure):
         ("steps", C.c_longlong),
         ("t", C.c_double),
         ("dt", C.c_double),
+        ("record_format", C.c_int),
+        ("step_kernels", C.c_int),
+        ("reorders", C.c_longlong),
+        ("order_kernels", C.c_int),
     ]
 
 

@@ -42,6 +42,9 @@ def build(with_reference: bool | None = None) -> None:
     targets = ["oracle"]
     if with_reference or (with_reference is None and os.path.isdir(ref_tree)):
         targets.append("ref")
+        # the reference's own driver linked against the engine library
+        if os.path.exists(os.path.join(HERE, "..", "n-body-code_b200", "lib", "libnbody_cuda.so")):
+            targets.append("ref_gpu")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_tree}", *targets], check=True,
                    stdout=subprocess.DEVNULL)
 

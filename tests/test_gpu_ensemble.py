@@ -53,7 +53,7 @@ def test_ensemble_mixed_matches_single_engine(small_ensemble):
         if n == 1:
             continue
         s = split(state, off, c)
-        with nb.Engine(int(n), eps2=eps2[c], precision="mixed", dt=1.0) as single:
+        with nb.Engine(int(n), eps2=eps2[c], precision="mixed", dt=1.0, pair_variant=3) as single:
             single.set_state(s)
             single.force_calculation()
             ref = single.get_derivs()

@@ -70,18 +70,31 @@ def test_fp64_every_tiling_agrees(tiling):
     assert ea <= TOL_FP64 and ej <= TOL_FP64, (tiling, ea, ej)
 
 
-@pytest.mark.parametrize("tiling", [dict(threads=128, i_per_thread=4, j_tile=128, split_j=1),
-                                    dict(threads=128, i_per_thread=2, j_tile=128, split_j=5),
-                                    dict(threads=256, i_per_thread=2, j_tile=128, split_j=2),
-                                    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64),
-                                    dict(threads=128, i_per_thread=4, j_tile=64, split_j=3),
-                                    dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
-                                    dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1),
-                                    dict(threads=128, i_per_thread=4, j_tile=128, split_j=9, pair_variant=2),
-                                    dict(threads=256, i_per_thread=4, j_tile=128, split_j=4),
-                                    dict(threads=128, i_per_thread=2, j_tile=128, split_j=11)])
+@pytest.mark.parametrize("tiling", [
+    # packed hi/lo, FP64 accumulators in shared memory (variant 3)
+    dict(threads=128, i_per_thread=4, j_tile=128, split_j=1, pair_variant=3),
+    dict(threads=128, i_per_thread=2, j_tile=128, split_j=5, pair_variant=3),
+    dict(threads=256, i_per_thread=2, j_tile=128, split_j=2, pair_variant=2),
+    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64, pair_variant=3),
+    dict(threads=128, i_per_thread=4, j_tile=64, split_j=3, pair_variant=3),
+    dict(threads=256, i_per_thread=4, j_tile=128, split_j=4, pair_variant=3),
+    dict(threads=128, i_per_thread=2, j_tile=128, split_j=11, pair_variant=3),
+    # scalar hi/lo (1), packed hi/lo with register accumulators (2)
+    dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
+    dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1),
+    dict(threads=128, i_per_thread=4, j_tile=128, split_j=9, pair_variant=2),
+    # tile-relative (0, the default)
+    dict(threads=128, i_per_thread=4, j_tile=128, split_j=1),
+    dict(threads=128, i_per_thread=2, j_tile=128, split_j=7),
+    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64),
+    dict(threads=256, i_per_thread=2, j_tile=128, split_j=3),
+    dict(threads=256, i_per_thread=4, j_tile=128, split_j=2),
+    dict(threads=128, i_per_thread=2, j_tile=64, split_j=5),
+    dict(threads=128, i_per_thread=4, j_tile=64, split_j=2),
+    dict(threads=128, i_per_thread=2, j_tile=256, split_j=2)])
 def test_mixed_every_kernel_agrees(tiling):
-    """Packed-pair and scalar mixed kernels, every shape: same accuracy class."""
+    """Tile-relative, packed hi/lo and scalar mixed kernels, every shape:
+    same accuracy class."""
     s = nb.plummer(3000, seed=5)
     ref = O.force(s, 1e-4)
     d = engine_derivs(s, 1e-4, precision="mixed", **tiling)
@@ -257,3 +270,103 @@ def test_max_size_sampled_rows(precision):
     ea, ej = derivs_rel(d[:, rows], ref)
     tol = TOL_FP64 if precision == "fp64" else 1e-5
     assert ea <= tol and ej <= 10 * tol, (precision, ea, ej)
+
+
+# ---------------------------------------------------------------------------
+# Tile-relative mixed kernel (pair_variant 0, the default): j-bodies in
+# Morton-ordered tiles, positions as float offsets from the tile centre.
+# ---------------------------------------------------------------------------
+REL = dict(pair_variant=0)
+HILO = dict(pair_variant=3)
+
+
+@pytest.mark.parametrize("case", ["plummer", "far_from_origin", "two_clusters"])
+def test_tile_relative_accuracy_vs_hilo(case):
+    """Tile-relative separations stay in the hi/lo kernel's accuracy class:
+    per-body acc error against the FP64 oracle within 3x of the hi/lo
+    kernel's (median) and within the mixed bounds, wherever the system sits."""
+    n, eps2 = 4096, 1e-4
+    s = nb.plummer(n, seed=2)
+    if case == "far_from_origin":      # float hi parts alone would lose ~10 bits here
+        for k in ("x", "y", "z"):
+            s[k] = s[k] + 1000.0
+    elif case == "two_clusters":       # a tight cluster 50 units from a wide one
+        t = nb.plummer(n, seed=3)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            s[k] = np.where(np.arange(n) % 2 == 0, s[k], 0.05 * t[k] + (50.0 if k == "x" else 0.0))
+    ref = O.force(s, eps2)
+    rel = engine_derivs(s, eps2, precision="mixed", **REL)
+    hilo = engine_derivs(s, eps2, precision="mixed", **HILO)
+    er, eh = vec_rel(rel[:3], ref[:3]), vec_rel(hilo[:3], ref[:3])
+    jr, jh = vec_rel(rel[3:], ref[3:]), vec_rel(hilo[3:], ref[3:])
+    print(f"{case}: acc median rel {np.median(er):.3e} hilo {np.median(eh):.3e}; "
+          f"max rel {er.max():.3e} hilo {eh.max():.3e}; jerk median rel {np.median(jr):.3e} "
+          f"hilo {np.median(jh):.3e}")
+    assert np.median(er) <= 2e-6 and er.max() <= 2e-4
+    assert np.median(er) <= 3 * np.median(eh) + 1e-8
+    assert np.median(jr) <= 3 * np.median(jh) + 1e-7
+
+
+@pytest.mark.parametrize("n", (1, 2, 33, 255, 257, 1000))
+def test_tile_relative_small_and_ragged(n):
+    """Padding slots and partly filled tiles (n not a multiple of the tile)."""
+    eps2 = 1e-4
+    s = nb.plummer(max(n, 2), seed=11)
+    s = {k: v[:n].copy() for k, v in s.items()}
+    d = engine_derivs(s, eps2, precision="mixed", **REL)
+    assert np.all(np.isfinite(d))
+    if n == 1:
+        assert np.all(d == 0)
+        return
+    ref = O.force(s, eps2)
+    ea = vec_rel(d[:3], ref[:3])
+    assert ea.max() <= 2e-4, ea.max()
+
+
+def test_tile_relative_deterministic_and_order_free():
+    """Bitwise reproducible (stable sort, fixed reduction order); the result
+    does not depend on the order the bodies are given in."""
+    n, eps2 = 5000, 1e-4
+    s = nb.plummer(n, seed=9)
+    a = engine_derivs(s, eps2, precision="mixed", **REL)
+    b = engine_derivs(s, eps2, precision="mixed", **REL)
+    assert np.array_equal(a, b)
+    perm = np.random.default_rng(0).permutation(n)
+    c = engine_derivs({k: v[perm] for k, v in s.items()}, eps2, precision="mixed", **REL)
+    ea, ej = derivs_rel(c, a[:, perm])
+    assert ea <= 1e-5 and ej <= 1e-4, (ea, ej)
+
+
+def test_tile_relative_device_entry_and_steps():
+    """Caller-owned device arrays (n below the engine's size), then Hermite
+    runs against the FP64 engine with the Morton order refreshed every step
+    and every 16 steps."""
+    import torch
+    n, eps2 = 3000, 1e-4
+    s = nb.plummer(n, seed=8)
+    m = n - 100
+    sub = {k: v[:m] for k, v in s.items()}
+    t = {k: torch.tensor(sub[k], dtype=torch.float64, device="cuda") for k in nb.FIELDS}
+    out = [torch.empty(m, dtype=torch.float64, device="cuda") for _ in range(6)]
+    with nb.Engine(n, eps2=eps2, precision="mixed", dt=1.0, **REL) as e:
+        e.acc_jerk_device(*[t[k] for k in nb.FIELDS], out, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        got = torch.stack(out).cpu().numpy()
+        # the engine's own system after a foreign call: its order is rebuilt
+        e.set_state(s)
+        e.force_calculation()
+        own = e.get_derivs()
+    ref = O.force(sub, eps2)
+    assert vec_rel(got[:3], ref[:3]).max() <= 2e-4
+    assert vec_rel(own[:3], O.force(s, eps2)[:3]).max() <= 2e-4
+    runs = {}
+    for name, prec, kw in (("fp64", "fp64", {}), ("rel1", "mixed", dict(REL, sort_every=1)),
+                           ("rel16", "mixed", REL)):
+        with nb.Engine(n, eps2=eps2, precision=prec, dt=1.0 / 1024, **kw) as e:
+            e.set_state(s)
+            e.force_calculation()
+            e.timestepping(40)
+            runs[name] = e.get_state()
+    for name in ("rel1", "rel16"):
+        dx = max(np.abs(runs[name][k] - runs["fp64"][k]).max() for k in ("x", "y", "z"))
+        assert dx <= 1e-8, (name, dx)
