@@ -123,10 +123,14 @@ const std::vector<PairKernel>& registry() {
       make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
       make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
       make_fp64<128, 2, 128, 1, 6>(), make_fp64<128, 2, 64, 1, 6>(), make_fp64<128, 1, 128, 4, 8>(),
-      // tile-relative packed pairs (Morton-ordered j-tiles; default mixed)
-      make_mixed_rel<128, 4, 128>(), make_mixed_rel<64, 4, 128>(),  make_mixed_rel<128, 2, 128>(),
+      // tile-relative packed pairs (Morton-ordered j-tiles; default mixed:
+      // 128 x 4 rows, j-unroll 2, 4 CTAs/SM = 128 registers, no spills)
+      make_mixed_rel<128, 4, 128, 1, 2, 4>(), make_mixed_rel<64, 4, 128>(), make_mixed_rel<128, 2, 128>(),
       make_mixed_rel<256, 2, 128>(), make_mixed_rel<256, 4, 128>(), make_mixed_rel<128, 2, 64>(),
       make_mixed_rel<128, 4, 64>(),  make_mixed_rel<128, 2, 256>(), make_mixed_rel<128, 4, 128, 0, 2>(),
+      make_mixed_rel<128, 4, 128>(), make_mixed_rel<128, 4, 128, 1, 1, 4>(),
+      make_mixed_rel<64, 4, 128, 1, 1, 8>(),  make_mixed_rel<128, 6, 128, 1, 1>(),
+      make_mixed_rel<64, 6, 128, 1, 1>(),     make_mixed_rel<128, 4, 128, 1, 2>(),
       // packed pairs, FP64 accumulators in shared memory (default)
       make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
       make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
