@@ -395,13 +395,15 @@ def main_ensemble(a):
     sizes, eps2, state = nb.plummer_ensemble(a.clusters, 3)
     dt = 1.0 / 512
     inter = float((sizes.astype(np.float64) ** 2).sum())
-    ens = nb.Ensemble(sizes, eps2, dt, precision=a.precision, tune=True)
+    variant = a.variant if a.precision == "mixed" else 0
+    ens = nb.Ensemble(sizes, eps2, dt, precision=a.precision, tune=True, pair_variant=variant)
     ens.set_state(state)
     ens.force_calculation()
     T0, U0 = ens.energy()
     stream = torch.cuda.ExternalStream(ens.stream, device=f"cuda:{dev}")
     ens.timestepping(a.warmup)
     ens.synchronize()
+    reorders0 = ens.info()["reorders"]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
     with torch.cuda.stream(stream), ClockSampler(dev) as clk:
         for k in range(a.steps):
@@ -411,6 +413,7 @@ def main_ensemble(a):
         ens.synchronize()
     ms = float(np.mean([s.elapsed_time(t) for s, t in ev]))
     info = ens.info()
+    launches = info["step_kernels"] * a.steps + info["order_kernels"] * (info["reorders"] - reorders0)
     de_run = None
     if a.time_units > 0:
         nsteps = int(round(a.time_units / dt)) - a.warmup - a.steps
@@ -425,8 +428,10 @@ def main_ensemble(a):
     engines = []
     off = np.concatenate([[0], np.cumsum(sizes)])
     for c, n in enumerate(sizes):
-        # the single-system engines run the ensemble kernel's pair arithmetic
-        # (packed hi/lo for mixed)
+        # the single-system engines use their fastest kernel at these sizes
+        # (256-8192 bodies): packed hi/lo for mixed (measured 163 vs 123 Gint/s
+        # serial for tile-relative engines, whose record building is a larger
+        # share of a small system's step)
         e = nb.Engine(int(n), eps2=float(eps2[c]), precision=a.precision, dt=dt,
                       pair_variant=3 if a.precision == "mixed" else 0)
         e.set_state({k: state[k][off[c]:off[c + 1]] for k in nb.FIELDS})
@@ -463,7 +468,8 @@ def main_ensemble(a):
                                f"eps = 4/N, dt = 1/512, {a.precision}",
                    "bodies": int(sizes.sum()), "interactions_per_step": inter,
                    "l2": "inputs larger than L2 (no flush)"},
-        "ensemble": {k: info[k] for k in ("items", "tiles_per_item", "j_tile", "threads", "grid", "padded_rows")},
+        "ensemble": {k: info[k] for k in ("items", "tiles_per_item", "j_tile", "threads", "grid", "padded_rows",
+                                          "record_format")},
         "launch_per_cluster_serial": {
             "ms_per_step": serial_ms, "value": inter / (serial_ms * 1e-3) / 1e9,
             "how": "one single-system engine per cluster stepped one at a time; sum of each "
@@ -476,7 +482,7 @@ def main_ensemble(a):
         "speedup_vs_launch_per_cluster_concurrent": base_ms / ms,
         "energy_error": de_run,
         "clocks": clk.summary(),
-        "gpu_launches": 3 * a.steps,
+        "gpu_launches": int(launches),
     }
     print(json.dumps(line), flush=True)
     return 0

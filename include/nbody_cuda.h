@@ -216,6 +216,10 @@ typedef struct {
   int tiles_per_item;    /* j-tiles per work item; 0 = default 8, or (with the
                             kernel shape) chosen by timing when tune = 1    */
   int tune;
+  int pair_variant;      /* mixed only: 0 = tile-relative packed kernel
+                            (per-cluster Morton tiles; default), 3 = packed
+                            hi/lo kernel (nbody_config numbering)          */
+  int sort_every;        /* variant 0: re-order every this many steps; 0 = 16 */
 } nbody_ensemble_config;
 typedef struct {
   int nclusters, padded_rows, items, tiles_per_item, grid;
@@ -223,6 +227,10 @@ typedef struct {
   double interactions_per_step;  /* sum of n[c]^2 */
   long long steps;
   double last_step_ms;           /* CUDA events around the last graph step */
+  int record_format;             /* as nbody_timers.record_format          */
+  int step_kernels;              /* kernel launches in one captured step   */
+  long long reorders;            /* Morton re-orderings run by steps       */
+  int order_kernels;             /* kernel launches in one re-ordering     */
 } nbody_ensemble_info_t;
 
 nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_config* cfg);

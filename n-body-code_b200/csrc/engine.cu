@@ -456,9 +456,9 @@ nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_
   JBodyRel* out = static_cast<JBodyRel*>(e->jb32);
   const int tiles = e->ld / tj;
   switch (tj) {
-    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(n, in, order, out); break;
-    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(n, in, order, out); break;
-    case 256: rel_tile_kernel<256><<<tiles, 256, 0, st>>>(n, in, order, out); break;
+    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(n, in, order, out, nullptr); break;
+    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(n, in, order, out, nullptr); break;
+    case 256: rel_tile_kernel<256><<<tiles, 256, 0, st>>>(n, in, order, out, nullptr); break;
     default: return fail(NBODY_ERR_INVALID_ARG, "no tile-relative record builder for j_tile %d", tj);
   }
   NB_CUDA(cudaGetLastError());

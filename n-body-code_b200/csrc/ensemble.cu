@@ -15,10 +15,16 @@
 // corrector, so results are bitwise reproducible.
 //
 // A step is memset(counter) -> predict -> persistent pair -> correct,
-// captured once into a CUDA graph.  Each cluster has its own softening and
+// captured once into a CUDA graph (mixed, tile-relative: the j-tile records
+// are rebuilt right after predict; every sort_every steps a second captured
+// graph re-orders each cluster's bodies along the Morton curve of its own
+// bounding box first - one global stable sort of (cluster, Morton code) keys,
+// which leaves every cluster in its own padded segment).  Each cluster has its own softening and
 // fixed shared step (the adaptive criterion is per system in the reference,
 // src/nbody.cpp:198-222; ensembles here run fixed steps).
 #include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -33,6 +39,7 @@
 #include "errors.h"
 #include "hermite.cuh"
 #include "pair.cuh"
+#include "reltiles.cuh"
 #include "trace.h"
 
 using namespace nbody;
@@ -109,6 +116,51 @@ __global__ void ens_predict_kernel(int L, const int* __restrict__ cid,
     jb64[r] = b;
   }
   if (jbx) jbx[r] = make_jbx2(p[0], p[1], p[2], m, u[0], u[1], u[2]);
+}
+
+// bbox[c*6 + k]: min (k < 3) / max of cluster c's positions (one CTA each).
+__global__ void __launch_bounds__(kBlock) ens_bbox_kernel(const ClusterDev* __restrict__ cl,
+                                                         const double* __restrict__ X, int L,
+                                                         double* __restrict__ bbox) {
+  __shared__ double sh[6 * 32];
+  const ClusterDev k = cl[blockIdx.x];
+  double v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (int i = threadIdx.x; i < k.n; i += blockDim.x) {
+    const int r = k.row0 + i;
+    const double x = X[r], y = X[L + r], z = X[2 * L + r];
+    v[0] = fmin(v[0], x); v[1] = fmin(v[1], y); v[2] = fmin(v[2], z);
+    v[3] = fmax(v[3], x); v[4] = fmax(v[4], y); v[5] = fmax(v[5], z);
+  }
+  block_minmax6(v, sh);
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    if (threadIdx.x == q) bbox[blockIdx.x * 6 + q] = v[q];
+}
+
+// keys[r] = (segment cluster << 48) | 48-bit Morton code (16 bits per axis)
+// in the cluster's box; padding rows take the segment's largest key, so the
+// sorted rows of cluster c fill exactly its padded segment, bodies first.
+__global__ void ens_key_kernel(int L, const int* __restrict__ cid, const int* __restrict__ seg,
+                               const double* __restrict__ X, const double* __restrict__ bbox,
+                               uint64_t* __restrict__ keys, int* __restrict__ vals) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= L) return;
+  const int c = seg[r];
+  uint64_t key = static_cast<uint64_t>(c) << 48;
+  if (cid[r] < 0) {
+    key |= 0xffffffffffffull;
+  } else {
+    constexpr double kCells = 65535.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double lo = bbox[c * 6 + k], w = bbox[c * 6 + 3 + k] - lo;
+      double q = w > 0.0 ? (X[k * L + r] - lo) * (kCells / w) : 0.0;
+      q = fmin(fmax(q, 0.0), kCells);  // NaN -> 0
+      key |= morton_spread21(static_cast<uint32_t>(q)) << k;
+    }
+  }
+  keys[r] = key;
+  vals[r] = r;
 }
 
 // Sum of a row's split partials, field f.
@@ -210,6 +262,7 @@ __global__ void ens_energy_sum_kernel(const ClusterDev* __restrict__ cl, const d
 // first of each precision is the default, the autotuner times all of them.
 struct EnsKernel {
   int precision, nt, tile;
+  int fmt;  // RecordFormat of its j-records
   const void* fn;
   size_t smem;
 };
@@ -217,14 +270,28 @@ struct EnsKernel {
 template <class R>
 EnsKernel ens_kernel(int precision) {
   static_assert(R::ROWS == kPadRows, "an item's row block is one padding unit");
-  return {precision, R::NT, R::TJ, reinterpret_cast<const void*>(&ensemble_pair_kernel<R>),
-          pair_smem_bytes<R>()};
+  return {precision, R::NT, R::TJ, precision == NBODY_FP64 ? kRecF64 : kRecX2,
+          reinterpret_cast<const void*>(&ensemble_pair_kernel<R>), pair_smem_bytes<R>()};
 }
 
+template <class R>
+EnsKernel ens_kernel_rel() {
+  static_assert(R::ROWS == kPadRows, "an item's row block is one padding unit");
+  return {NBODY_MIXED, R::NT, R::TJ, kRecRel,
+          reinterpret_cast<const void*>(&ensemble_pair_rel_kernel<R>),
+          2 * (R::TJ + 1) * sizeof(JBodyRel) + R::kExtraSmem};
+}
+
+// The first entry of each (precision, record format) is its default.
 const std::vector<EnsKernel>& ens_registry() {
   static const std::vector<EnsKernel> r = {
       ens_kernel<RowsFP64<128, 2, 128, 1>>(NBODY_FP64),
       ens_kernel<RowsFP64<256, 1, 128, 4>>(NBODY_FP64),
+      ens_kernel_rel<RowsMixedRel<64, 4, 64, 1, 1>>(),
+      ens_kernel_rel<RowsMixedRel<64, 4, 128, 1, 1>>(),
+      ens_kernel_rel<RowsMixedRel<128, 2, 128, 1, 1>>(),
+      ens_kernel_rel<RowsMixedRel<128, 2, 64, 1, 1>>(),
+      ens_kernel_rel<RowsMixedRel<64, 4, 64, 1, 2>>(),
       ens_kernel<RowsMixedX2<64, 4, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<128, 2, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<64, 4, 64, 1, 1>>(NBODY_MIXED),
@@ -236,6 +303,7 @@ const std::vector<EnsKernel>& ens_registry() {
 
 struct nbody_ensemble {
   int C = 0, L = 0, dev = 0, sms = 0, precision = 0;
+  int fmt = kRecF64;  // record format of the pair kernels in use
   int tiles_per_item = 8;
   const EnsKernel* kern = nullptr;  // persistent pair kernel in use
   int grid = 0;
@@ -259,9 +327,21 @@ struct nbody_ensemble {
   int n_blk = 0;
   double *phi = nullptr, *Tc = nullptr, *Uc = nullptr;
   cudaGraphExec_t graph = nullptr;
+  int step_kernels = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool have_derivs = false;
   long long steps = 0;
+  // Morton ordering of the tile-relative records (mixed, variant 0)
+  int* seg = nullptr;             // [L] cluster owning each padded row
+  double* bbox = nullptr;         // [C][6]
+  uint64_t* sort_keys = nullptr;  // [2][L]
+  int* sort_idx = nullptr;        // [2][L]; second half = order
+  void* sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
+  int sort_bits = 49, sort_every = 16, since_sort = 0;
+  cudaGraphExec_t order_graph = nullptr;
+  int order_kernels = 0;
+  long long reorders = 0;
 };
 
 namespace {
@@ -327,10 +407,41 @@ nbody_status launch_ens_pair(nbody_ensemble* e) {
   EN_CUDA(cudaMemsetAsync(e->counter, 0, sizeof(unsigned int), e->stream));
   const bool fp64 = e->precision == NBODY_FP64;
   const void* jb = fp64 ? static_cast<const void*>(e->jb64) : static_cast<const void*>(e->jbx);
+  const size_t L = e->L;
+  RowSrc rows{e->X, e->X + L, e->X + 2 * L, e->V, e->V + L, e->V + 2 * L};
   void* args[] = {const_cast<void*>(static_cast<const void*>(&jb)), &e->items, &e->n_items,
-                  &e->counter, &e->P, &e->status};
+                  &e->counter, &e->P, &e->status, &rows};
   EN_CUDA(cudaLaunchKernel(e->kern->fn, dim3(e->grid), dim3(e->kern->nt), args, e->kern->smem,
                            e->stream));
+  return NBODY_OK;
+}
+
+// Morton order of every cluster's bodies within its padded segment.
+nbody_status ens_order(nbody_ensemble* e, cudaStream_t st) {
+  ens_bbox_kernel<<<e->C, kBlock, 0, st>>>(e->cl, e->X, e->L, e->bbox);
+  ens_key_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, st>>>(e->L, e->cid, e->seg, e->X,
+                                                                  e->bbox, e->sort_keys, e->sort_idx);
+  EN_CUDA(cudaGetLastError());
+  const size_t L = e->L;
+  size_t bytes = e->sort_tmp_bytes;
+  EN_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + L,
+                                          e->sort_idx, e->sort_idx + L, e->L, 0, e->sort_bits, st));
+  return NBODY_OK;
+}
+
+// Tile-relative records (tiles of the kernel's TJ) in the last order.
+nbody_status ens_tiles(nbody_ensemble* e, cudaStream_t st) {
+  const size_t L = e->L;
+  const SoA7 in{e->X, e->X + L, e->X + 2 * L, e->M, e->V, e->V + L, e->V + 2 * L};
+  const int* order = e->sort_idx + L;
+  JBodyRel* out = reinterpret_cast<JBodyRel*>(e->jbx);
+  const int tiles = e->L / e->kern->tile;
+  switch (e->kern->tile) {
+    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(e->L, in, order, out, e->cid); break;
+    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(e->L, in, order, out, e->cid); break;
+    default: return nbody_set_error(NBODY_ERR_INVALID_ARG, "no record builder for tile %d", e->kern->tile);
+  }
+  EN_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
 
@@ -347,11 +458,30 @@ nbody_status use_kernel(nbody_ensemble* e, const EnsKernel* k) {
 }
 
 nbody_status launch_ens_pack(nbody_ensemble* e) {
-  const bool fp64 = e->precision == NBODY_FP64;
   ens_pack_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
-      e->L, e->cid, e->X, e->V, e->M, e->jb64, fp64 ? nullptr : e->jbx);
+      e->L, e->cid, e->X, e->V, e->M, e->jb64, e->fmt == kRecX2 ? e->jbx : nullptr);
   EN_CUDA(cudaGetLastError());
+  if (e->fmt == kRecRel) {
+    EN_TRY(ens_order(e, e->stream));
+    e->since_sort = 0;
+    EN_TRY(ens_tiles(e, e->stream));
+  }
   return NBODY_OK;
+}
+
+int count_graph_kernels(cudaGraph_t g) {
+  size_t nodes = 0;
+  int kernels = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+    std::vector<cudaGraphNode_t> v(nodes);
+    if (cudaGraphGetNodes(g, v.data(), &nodes) == cudaSuccess)
+      for (size_t k = 0; k < nodes; ++k) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(v[k], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel)
+          ++kernels;
+      }
+  }
+  return kernels;
 }
 
 nbody_status ens_eval_current(nbody_ensemble* e) {
@@ -374,7 +504,8 @@ nbody_status ens_build_graph(nbody_ensemble* e) {
     s = nbody_set_error(NBODY_ERR_CUDA, "event record during capture failed");
   ens_predict_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
       e->L, e->cid, e->cl, e->X, e->V, e->M, e->D, fp64 ? e->jb64 : nullptr,
-      fp64 ? nullptr : e->jbx);
+      e->fmt == kRecX2 ? e->jbx : nullptr);
+  if (s == NBODY_OK && e->fmt == kRecRel) s = ens_tiles(e, e->stream);
   if (s == NBODY_OK) s = launch_ens_pair(e);
   ens_correct_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->cid, e->cl,
                                                                            e->P, e->X, e->V, e->D);
@@ -386,11 +517,30 @@ nbody_status ens_build_graph(nbody_ensemble* e) {
     return s;
   }
   if (ce != cudaSuccess) return nbody_set_error(NBODY_ERR_CUDA, "capture: %s", cudaGetErrorString(ce));
+  e->step_kernels = count_graph_kernels(g);
   ce = cudaGraphInstantiate(&e->graph, g, 0);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) {
     e->graph = nullptr;
     return nbody_set_error(NBODY_ERR_CUDA, "instantiate: %s", cudaGetErrorString(ce));
+  }
+  if (e->fmt == kRecRel && !e->order_graph) {
+    EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    s = ens_order(e, e->stream);
+    g = nullptr;
+    ce = cudaStreamEndCapture(e->stream, &g);
+    if (s != NBODY_OK) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    if (ce != cudaSuccess) return nbody_set_error(NBODY_ERR_CUDA, "capture: %s", cudaGetErrorString(ce));
+    e->order_kernels = count_graph_kernels(g);
+    ce = cudaGraphInstantiate(&e->order_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      e->order_graph = nullptr;
+      return nbody_set_error(NBODY_ERR_CUDA, "instantiate: %s", cudaGetErrorString(ce));
+    }
   }
   return NBODY_OK;
 }
@@ -406,8 +556,9 @@ nbody_status ens_autotune(nbody_ensemble* e) {
   const EnsKernel* best_k = e->kern;
   int best_tpi = 8;
   for (const EnsKernel& k : ens_registry()) {
-    if (k.precision != e->precision) continue;
+    if (k.precision != e->precision || k.fmt != e->fmt) continue;
     EN_TRY(use_kernel(e, &k));
+    if (e->fmt == kRecRel) EN_TRY(ens_tiles(e, e->stream));  // this kernel's tile size
     for (int j_per_item : {256, 512, 1024, 2048, 4096, 8192}) {
       const int tpi = std::max(1, j_per_item / k.tile);
       EN_TRY(build_items(e, tpi));
@@ -432,6 +583,7 @@ nbody_status ens_autotune(nbody_ensemble* e) {
   cudaEventDestroy(b);
   EN_TRY(ens_status(e));
   EN_TRY(use_kernel(e, best_k));
+  if (e->fmt == kRecRel) EN_TRY(ens_tiles(e, e->stream));
   return build_items(e, best_tpi);
 }
 
@@ -450,10 +602,12 @@ nbody_status nbody_ensemble_destroy(nbody_ensemble* e) {
   cudaSetDevice(e->dev);
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->order_graph) cudaGraphExecDestroy(e->order_graph);
   for (auto ev : e->ev)
     if (ev) cudaEventDestroy(ev);
   void* bufs[] = {e->state, e->P, e->jb64, e->jbx, e->cid, e->cl, e->items, e->counter,
-                  e->status, e->blk_cluster, e->blk_row, e->phi, e->Tc, e->Uc};
+                  e->status, e->blk_cluster, e->blk_row, e->phi, e->Tc, e->Uc,
+                  e->seg, e->bbox, e->sort_keys, e->sort_idx, e->sort_tmp};
   for (void* p : bufs) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -469,6 +623,14 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
   if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
   if (cfg->tiles_per_item < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "tiles_per_item < 0");
+  if (cfg->precision == NBODY_MIXED && cfg->pair_variant != 0 && cfg->pair_variant != 3)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG,
+                           "ensemble pair_variant = %d (0 tile-relative, 3 packed hi/lo)", cfg->pair_variant);
+  if (cfg->sort_every < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "sort_every < 0");
+  const bool rel = cfg->precision == NBODY_MIXED && cfg->pair_variant == 0;
+  if (rel && C > 65536)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG,
+                           "tile-relative ensembles hold at most 65536 clusters (use pair_variant 3)");
   long long L = 0;
   for (int c = 0; c < C; ++c) {
     if (cfg->n[c] < 1) return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d has n = %d", c, cfg->n[c]);
@@ -493,17 +655,21 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
   e->L = static_cast<int>(L);
   e->dev = cfg->device;
   e->precision = cfg->precision;
+  e->fmt = cfg->precision == NBODY_FP64 ? kRecF64 : (rel ? kRecRel : kRecX2);
+  e->sort_every = cfg->sort_every > 0 ? cfg->sort_every : 16;
+  while ((1LL << (e->sort_bits - 48)) < C) ++e->sort_bits;  // cluster id above the 48-bit code
   cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->dev);
   e->n.assign(cfg->n, cfg->n + C);
   e->eps2.assign(cfg->eps2, cfg->eps2 + C);
   e->dt.assign(cfg->dt, cfg->dt + C);
-  std::vector<int> cid(e->L, -1), blk_cluster, blk_row;
+  std::vector<int> cid(e->L, -1), seg(e->L, 0), blk_cluster, blk_row;
   int r0 = 0;
   for (int c = 0; c < C; ++c) {
     const int ld = (e->n[c] + kPadRows - 1) / kPadRows * kPadRows;
     e->row0.push_back(r0);
     e->ld.push_back(ld);
     for (int i = 0; i < e->n[c]; ++i) cid[r0 + i] = c;
+    for (int i = 0; i < ld; ++i) seg[r0 + i] = c;
     for (int b = 0; b < ld; b += kPadRows) {
       blk_cluster.push_back(c);
       blk_row.push_back(b);
@@ -537,9 +703,22 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     EN_CUDA(cudaMalloc(&raw->phi, sizeof(double) * Ls));
     EN_CUDA(cudaMalloc(&raw->Tc, sizeof(double) * raw->C));
     EN_CUDA(cudaMalloc(&raw->Uc, sizeof(double) * raw->C));
+    if (raw->fmt == kRecRel) {
+      static_assert(sizeof(JBodyX2) >= sizeof(JBodyRel) * 65 / 64, "jbx holds tiles of >= 64");
+      EN_CUDA(cudaMalloc(&raw->seg, sizeof(int) * Ls));
+      EN_CUDA(cudaMemcpy(raw->seg, seg.data(), sizeof(int) * Ls, cudaMemcpyHostToDevice));
+      EN_CUDA(cudaMalloc(&raw->bbox, sizeof(double) * 6 * raw->C));
+      EN_CUDA(cudaMalloc(&raw->sort_keys, sizeof(uint64_t) * 2 * Ls));
+      EN_CUDA(cudaMalloc(&raw->sort_idx, sizeof(int) * 2 * Ls));
+      EN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, raw->sort_tmp_bytes, raw->sort_keys,
+                                              raw->sort_keys + Ls, raw->sort_idx,
+                                              raw->sort_idx + Ls, raw->L, 0, raw->sort_bits,
+                                              raw->stream));
+      EN_CUDA(cudaMalloc(&raw->sort_tmp, std::max<size_t>(raw->sort_tmp_bytes, 16)));
+    }
     for (auto& ev : raw->ev) EN_CUDA(cudaEventCreate(&ev));
     for (const EnsKernel& k : ens_registry())
-      if (k.precision == raw->precision) {
+      if (k.precision == raw->precision && k.fmt == raw->fmt) {
         EN_TRY(use_kernel(raw, &k));
         break;
       }
@@ -627,7 +806,15 @@ nbody_status nbody_ensemble_step(nbody_ensemble* e, int nsteps) {
   if (nsteps < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "nsteps < 0");
   if (!e->have_derivs) EN_TRY(ens_eval_current(e));
   EN_TRY(ens_build_graph(e));
-  for (int k = 0; k < nsteps; ++k) EN_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    if (e->fmt == kRecRel && e->since_sort >= e->sort_every) {
+      EN_CUDA(cudaGraphLaunch(e->order_graph, e->stream));
+      e->since_sort = 0;
+      ++e->reorders;
+    }
+    EN_CUDA(cudaGraphLaunch(e->graph, e->stream));
+    ++e->since_sort;
+  }
   e->steps += nsteps;
   return NBODY_OK;
 }
@@ -669,6 +856,10 @@ nbody_status nbody_ensemble_info(nbody_ensemble* e, nbody_ensemble_info_t* out) 
   float ms = 0;
   if (e->graph && cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]) == cudaSuccess) out->last_step_ms = ms;
   cudaGetLastError();
+  out->record_format = e->fmt;
+  out->step_kernels = e->step_kernels;
+  out->reorders = e->reorders;
+  out->order_kernels = e->order_kernels;
   return NBODY_OK;
 }
 

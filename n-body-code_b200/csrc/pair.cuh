@@ -686,6 +686,46 @@ __device__ __forceinline__ void pair_ensemble(const typename R::JB* __restrict__
   }
 }
 
+// Tile-relative ensemble: tiles of TJ + 1 records over the whole padded
+// array (cluster segments are multiples of 256 rows, so a tile never spans
+// two clusters); i-rows from the FP64 state `rows` (padded row order).
+template <class R>
+__device__ __forceinline__ void pair_ensemble_rel(const JBodyRel* __restrict__ jt,
+                                                  const EnsItem* __restrict__ items, int n_items,
+                                                  unsigned int* counter, double* P, int* status,
+                                                  const RowSrc& rows, unsigned char* smem,
+                                                  uint64_t* full, int* s_item) {
+  constexpr int kRecs = R::TJ + 1;
+  TilePipe<JBodyRel, kRecs> pipe;
+  pipe.init(reinterpret_cast<JBodyRel*>(smem), full);
+  for (;;) {
+    if (threadIdx.x == 0) *s_item = static_cast<int>(atomicAdd(counter, 1u));
+    __syncthreads();
+    const int k = *s_item;
+    __syncthreads();
+    if (k >= n_items) return;
+    const EnsItem it = items[k];
+    const int row = it.row0 + threadIdx.x;  // cluster-relative
+    const RowSrc src{rows.x + it.jrow0, rows.y + it.jrow0, rows.z + it.jrow0,
+                     rows.vx + it.jrow0, rows.vy + it.jrow0, rows.vz + it.jrow0};
+    R r;
+    r.begin_rows(src, row, it.ld - 1, it.eps2, smem + 2 * kRecs * sizeof(JBodyRel));
+    const JBodyRel* ct = jt + static_cast<size_t>(it.jrow0 / R::TJ + it.t_begin) * kRecs;
+    if (!pipe.run(ct, it.nt, status, [&](const JBodyRel* tile) { r.consume(tile); })) return;
+    r.store(P + it.out_off, static_cast<size_t>(it.ld), row, it.rows_end);
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(R::NT) ensemble_pair_rel_kernel(
+    const JBodyRel* __restrict__ jt, const EnsItem* __restrict__ items, int n_items,
+    unsigned int* counter, double* P, int* status, RowSrc rows) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t full[2];
+  __shared__ int s_item;
+  pair_ensemble_rel<R>(jt, items, n_items, counter, P, status, rows, smem_raw, full, &s_item);
+}
+
 template <class R>
 __global__ void __launch_bounds__(R::NT) ensemble_pair_kernel(const typename R::JB* __restrict__ jb,
                                                               const EnsItem* __restrict__ items,

@@ -108,7 +108,8 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
 }
 
 // Tile t (CTA t, TJ threads) = header + the bodies order[t*TJ + k], k < TJ
-// (slots >= n are zero-mass padding at the centre).
+// (slots >= n, and rows with cid[row] < 0 when cid is given, are zero-mass
+// padding at the centre).
 //
 // Centre c = the per-axis median of the tile's positions, rounded to float
 // (a tile that straddles a jump of the Morton curve keeps its centre with
@@ -118,13 +119,15 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
 // therefore cancels exactly (r_ii = -D + D = 0), whatever the rounding.
 template <int TJ>
 __global__ void __launch_bounds__(TJ) rel_tile_kernel(int n, SoA7 in, const int* __restrict__ order,
-                                                      JBodyRel* __restrict__ out) {
+                                                      JBodyRel* __restrict__ out,
+                                                      const int* __restrict__ cid) {
   __shared__ double sp[3][TJ];
+  __shared__ int sv[TJ];
   __shared__ double med[3];
   const int tid = threadIdx.x;
   const int slot = blockIdx.x * TJ + tid;
-  const int nv = max(0, min(TJ, n - static_cast<int>(blockIdx.x) * TJ));  // valid slots: [0, nv)
-  const int b = tid < nv ? order[slot] : -1;
+  int b = slot < n ? order[slot] : -1;
+  if (b >= 0 && cid && cid[b] < 0) b = -1;
   double p[3] = {0.0, 0.0, 0.0}, m = 0, vx = 0, vy = 0, vz = 0;
   if (b >= 0) {
     p[0] = in.x[b]; p[1] = in.y[b]; p[2] = in.z[b]; m = in.m[b];
@@ -132,15 +135,16 @@ __global__ void __launch_bounds__(TJ) rel_tile_kernel(int n, SoA7 in, const int*
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) sp[k][tid] = p[k];
+  sv[tid] = b >= 0;
   if (tid < 3) med[tid] = 0.0;
-  __syncthreads();
+  const int nv = __syncthreads_count(b >= 0);
   if (b >= 0) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {  // rank of p[k] among the valid slots (ties by slot)
       int r = 0;
-      for (int q = 0; q < nv; ++q) {
+      for (int q = 0; q < TJ; ++q) {
         const double w = sp[k][q];
-        r += (w < p[k] || (w == p[k] && q < tid)) ? 1 : 0;
+        r += (sv[q] && (w < p[k] || (w == p[k] && q < tid))) ? 1 : 0;
       }
       if (r == nv / 2) med[k] = p[k];
     }

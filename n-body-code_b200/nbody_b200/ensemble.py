@@ -15,14 +15,16 @@ from .engine import FIELDS, PRECISIONS, _ptr, plummer
 class EnsembleConfig(C.Structure):
     _fields_ = [("nclusters", C.c_int), ("n", C.POINTER(C.c_int)), ("eps2", C.POINTER(C.c_double)),
                 ("dt", C.POINTER(C.c_double)), ("precision", C.c_int), ("device", C.c_int),
-                ("tiles_per_item", C.c_int), ("tune", C.c_int)]
+                ("tiles_per_item", C.c_int), ("tune", C.c_int), ("pair_variant", C.c_int),
+                ("sort_every", C.c_int)]
 
 
 class EnsembleInfo(C.Structure):
     _fields_ = [("nclusters", C.c_int), ("padded_rows", C.c_int), ("items", C.c_int),
                 ("tiles_per_item", C.c_int), ("grid", C.c_int), ("threads", C.c_int),
                 ("j_tile", C.c_int), ("interactions_per_step", C.c_double), ("steps", C.c_longlong),
-                ("last_step_ms", C.c_double)]
+                ("last_step_ms", C.c_double), ("record_format", C.c_int), ("step_kernels", C.c_int),
+                ("reorders", C.c_longlong), ("order_kernels", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -49,7 +51,8 @@ class Ensemble:
     """Clusters of sizes n[c] with softening eps2[c] and fixed step dt[c]."""
 
     def __init__(self, n, eps2, dt, precision: str = "mixed", device: int = 0,
-                 tiles_per_item: int = 0, tune: bool = False):
+                 tiles_per_item: int = 0, tune: bool = False, pair_variant: int = 0,
+                 sort_every: int = 0):
         self.n = np.ascontiguousarray(n, dtype=np.int32)
         C_ = self.n.size
         self.eps2 = np.ascontiguousarray(np.broadcast_to(eps2, (C_,)), dtype=np.float64)
@@ -57,7 +60,8 @@ class Ensemble:
         cfg = EnsembleConfig(C_, self.n.ctypes.data_as(C.POINTER(C.c_int)),
                              self.eps2.ctypes.data_as(C.POINTER(C.c_double)),
                              self.dt.ctypes.data_as(C.POINTER(C.c_double)),
-                             PRECISIONS[precision], device, tiles_per_item, int(tune))
+                             PRECISIONS[precision], device, tiles_per_item, int(tune),
+                             pair_variant, sort_every)
         h = _vp()
         check(_f("nbody_ensemble_create")(C.byref(h), C.byref(cfg)), "nbody_ensemble_create")
         self._h = h

@@ -43,8 +43,10 @@ def test_ensemble_fp64_forces_vs_oracle(small_ensemble, tpi):
 
 
 def test_ensemble_mixed_matches_single_engine(small_ensemble):
+    """Packed hi/lo kernels (pair_variant 3): the same pair arithmetic as the
+    single-system engine's, so agreement to the reordering of split sums."""
     sizes, eps2, state = small_ensemble
-    with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed", tiles_per_item=4) as e:
+    with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed", tiles_per_item=4, pair_variant=3) as e:
         e.set_state(state)
         e.force_calculation()
         d = e.get_derivs()
@@ -115,3 +117,52 @@ def test_plummer_ensemble_config():
     assert np.all(np.isfinite(de["mixed"]))
     assert np.all(de["mixed"] <= 2.0 * de["fp64"] + 1e-9), np.max(de["mixed"] / (de["fp64"] + 1e-12))
     assert info["tiles_per_item"] * info["j_tile"] in (256, 512, 1024, 2048, 4096, 8192)
+
+
+@pytest.mark.parametrize("tpi", [1, 4, 64])
+def test_ensemble_tile_relative_vs_oracle(small_ensemble, tpi):
+    """Tile-relative ensemble (the mixed default): per cluster against the FP64
+    oracle within the mixed bounds, and within 3x of the hi/lo ensemble's
+    median error."""
+    sizes, eps2, state = small_ensemble
+    d = {}
+    for name, kw in (("rel", {}), ("hilo", dict(pair_variant=3))):
+        with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed", tiles_per_item=tpi, **kw) as e:
+            e.set_state(state)
+            e.force_calculation()
+            d[name] = e.get_derivs()
+            off = e.offsets
+            info = e.info()
+            if name == "rel":
+                assert info["record_format"] == 3
+    for c, n in enumerate(sizes):
+        rel = d["rel"][:, off[c]:off[c + 1]]
+        assert np.all(np.isfinite(rel))
+        if n == 1:
+            assert np.all(rel == 0)
+            continue
+        ref = O.force(split(state, off, c), eps2[c])
+        er = vec_rel(rel[:3], ref[:3])
+        eh = vec_rel(d["hilo"][:3, off[c]:off[c + 1]], ref[:3])
+        assert np.median(er) <= 2e-6 and er.max() <= 2e-4, (c, n, np.median(er), er.max())
+        assert np.median(er) <= 3 * np.median(eh) + 1e-8, (c, n, np.median(er), np.median(eh))
+
+
+def test_ensemble_tile_relative_steps_vs_fp64(small_ensemble):
+    """16 steps with the order refreshed every step and every 16 steps: every
+    cluster stays within mixed-precision distance of the FP64 ensemble."""
+    sizes, eps2, state = small_ensemble
+    runs = {}
+    for name, prec, kw in (("fp64", "fp64", {}), ("rel1", "mixed", dict(sort_every=1)),
+                           ("rel", "mixed", {})):
+        with nb.Ensemble(sizes, eps2, 1 / 512, precision=prec, **kw) as e:
+            e.set_state(state)
+            e.timestepping(16)
+            runs[name] = e.get_state()
+            info = e.info()
+            if name == "rel1":
+                # the first step uses the order made with the initial forces
+                assert info["reorders"] == 15 and info["order_kernels"] >= 3
+    for name in ("rel1", "rel"):
+        dx = max(np.abs(runs[name][k] - runs["fp64"][k]).max() for k in ("x", "y", "z"))
+        assert dx <= 1e-7, (name, dx)
