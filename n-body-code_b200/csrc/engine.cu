@@ -51,6 +51,7 @@ constexpr int kPad = 256;        // body padding granularity (multiple of every 
 constexpr int kMaxSplit = 64;    // split-j upper bound
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
 constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
+constexpr int kMortonBits = 48;     // Morton key width (morton_key_kernel)
 
 thread_local std::string g_last_error;
 
@@ -443,7 +444,7 @@ nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaSt
   NB_CUDA(cudaGetLastError());
   size_t bytes = e->sort_tmp_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + ld,
-                                          e->sort_idx, e->sort_idx + ld, n, 0, 63, st));
+                                          e->sort_idx, e->sort_idx + ld, n, 0, kMortonBits, st));
   e->order_own = own && n == e->n;
   e->since_sort = 0;
   return NBODY_OK;
@@ -724,7 +725,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
       NB_CUDA(cudaMalloc(&e->bbox_part, sizeof(double) * 6 * kMaxBBoxParts));
       NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, e->sort_tmp_bytes, e->sort_keys,
                                               e->sort_keys + ld, e->sort_idx, e->sort_idx + ld,
-                                              static_cast<int>(ld), 0, 63, e->stream));
+                                              static_cast<int>(ld), 0, kMortonBits, e->stream));
       NB_CUDA(cudaMalloc(&e->sort_tmp, std::max<size_t>(e->sort_tmp_bytes, 16)));
     }
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));

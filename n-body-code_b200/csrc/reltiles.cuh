@@ -5,7 +5,7 @@
 // tile then stores its bodies as float offsets from the tile's centre.
 //
 //   bbox_partial_kernel   per-CTA min/max of x, y, z          (O(N) read, 24 B/body)
-//   morton_key_kernel     63-bit key (21 bits per axis) + index (O(N), 24 B in, 12 B out)
+//   morton_key_kernel     48-bit key (16 bits per axis) + index (O(N), 24 B in, 12 B out)
 //   (stable radix sort of (key, index) pairs: cub::DeviceRadixSort)
 //   rel_tile_kernel<TJ>   gather by sorted index, median tile centre, records
 //                         (O(N), 56 B gathered, 64 B written per body)
@@ -93,7 +93,7 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
   block_minmax6(v, sh);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  constexpr double kCells = 2097151.0;  // 2^21 - 1
+  constexpr double kCells = 65535.0;  // 2^16 - 1 cells per axis: a 48-bit key
   const double p[3] = {in.x[i], in.y[i], in.z[i]};
   uint64_t key = 0;
 #pragma unroll
