@@ -221,6 +221,8 @@ struct nbody_engine {
   cudaGraphExec_t graph = nullptr;
   int graph_kernels = 0;  // kernel nodes of the captured step
   cudaGraphExec_t order_graph = nullptr;  // captured Morton re-ordering (variant 0)
+  cudaStream_t aux = nullptr;              // drop-in: uploads that overlap the ordering
+  cudaEvent_t aux_ev[2] = {nullptr, nullptr};
   int order_kernels = 0;
   long long reorders = 0;  // re-orderings run before steps
   bool have_state = false, have_derivs = false;
@@ -466,16 +468,17 @@ nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_
   return NBODY_OK;
 }
 
-// Writes the FP64 records (always: the potential reads them) and, for a
-// mixed kernel, the records in that kernel's format (tiles of tj bodies;
-// tile-relative records are re-ordered first).
+// Writes the j-records of a pair kernel's format: FP64 records (hi/lo
+// kernels: also theirs), or tiles of tj tile-relative records, re-ordered
+// first.  (The energy diagnostic packs its own records.)
 nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
                          int tj) {
-  pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      n, e->ld, in, e->jb64, fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
-      fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
-  NB_CUDA(cudaGetLastError());
-  if (fmt == kRecRel) {
+  if (fmt != kRecRel) {
+    pack_kernel<<<(e->ld + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+        n, e->ld, in, e->jb64, fmt == kRecF32 ? static_cast<JBody32*>(e->jb32) : nullptr,
+        fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
+    NB_CUDA(cudaGetLastError());
+  } else {
     NB_TRY(enqueue_morton_order(e, n, in, st, in.x == e->X));
     NB_TRY(build_rel_tiles(e, n, in, st, tj));
   }
@@ -746,6 +749,9 @@ nbody_status nbody_destroy(nbody_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
   if (e->order_graph) cudaGraphExecDestroy(e->order_graph);
+  for (auto ev : e->aux_ev)
+    if (ev) cudaEventDestroy(ev);
+  if (e->aux) cudaStreamDestroy(e->aux);
   for (auto ev : e->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto ev : e->ev_init)
@@ -1025,13 +1031,32 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   const size_t ld = e->ld, b = sizeof(double) * n;
   const double* src[7] = {x, y, z, vx, vy, vz, m};
   double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};
-  for (int k = 0; k < 7; ++k)
-    NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
   NB_TRY(ensure_tiling(e));
   Tiling t = e->tiling;
   if (i_end - i_begin != n) NB_TRY(get_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
-  NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt, t.k->tj));
+  if (t.k->fmt == kRecRel) {
+    // positions first: their Morton ordering runs while the masses and
+    // velocities upload on a second stream
+    if (!e->aux) {
+      NB_CUDA(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
+      for (auto& ev : e->aux_ev) NB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    NB_CUDA(cudaEventRecord(e->aux_ev[0], e->stream));
+    NB_CUDA(cudaStreamWaitEvent(e->aux, e->aux_ev[0], 0));
+    for (int k = 0; k < 3; ++k)
+      NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
+    for (int k = 3; k < 7; ++k)
+      NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->aux));
+    NB_CUDA(cudaEventRecord(e->aux_ev[1], e->aux));
+    NB_TRY(enqueue_morton_order(e, n, own_inputs(e), e->stream, true));
+    NB_CUDA(cudaStreamWaitEvent(e->stream, e->aux_ev[1], 0));
+    NB_TRY(build_rel_tiles(e, n, own_inputs(e), e->stream, t.k->tj));
+  } else {
+    for (int k = 0; k < 7; ++k)
+      NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
+    NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt, t.k->tj));
+  }
   NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
   if (i_end > i_begin) {
     reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
@@ -1046,8 +1071,7 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     if (rb) NB_CUDA(cudaMemcpyAsync(out[k] + i_begin, e->D + k * ld + i_begin, rb,
                                     cudaMemcpyDeviceToHost, e->stream));
   }
-  NB_CUDA(cudaStreamSynchronize(e->stream));
-  return check_status_word(e);
+  return check_status_word(e);  // its read-back follows the outputs; one wait for all
 }
 
 extern "C" nbody_status nbody_force_calculation_release(void) {
