@@ -111,9 +111,11 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
 // (slots >= n, and rows with cid[row] < 0 when cid is given, are zero-mass
 // padding at the centre).
 //
-// Centre c = the per-axis median of the tile's positions, rounded to float
-// (a tile that straddles a jump of the Morton curve keeps its centre with
-// the majority of its bodies).  A body's stored offset is -D, with
+// Centre c = the per-axis median of up to 32 evenly spaced bodies of the
+// tile, rounded to float (a tile that straddles a jump of the Morton curve
+// keeps its centre with the majority of its bodies).  The valid slots of a
+// tile are a prefix (padding sorts last), so the samples are slots
+// floor(j * nv / 32); warp 0 ranks them with shuffles.  A body's stored offset is -D, with
 // D = fl(fl(c - x_hi) - x_lo) the very float operations the pair kernel
 // applies to an i-row (x_hi = fl(x), x_lo = fl(x - x_hi)); the self pair
 // therefore cancels exactly (r_ii = -D + D = 0), whatever the rounding.
@@ -121,8 +123,6 @@ template <int TJ>
 __global__ void __launch_bounds__(TJ) rel_tile_kernel(int n, SoA7 in, const int* __restrict__ order,
                                                       JBodyRel* __restrict__ out,
                                                       const int* __restrict__ cid) {
-  __shared__ double sp[3][TJ];
-  __shared__ int sv[TJ];
   __shared__ double med[3];
   const int tid = threadIdx.x;
   const int slot = blockIdx.x * TJ + tid;
@@ -133,20 +133,25 @@ __global__ void __launch_bounds__(TJ) rel_tile_kernel(int n, SoA7 in, const int*
     p[0] = in.x[b]; p[1] = in.y[b]; p[2] = in.z[b]; m = in.m[b];
     vx = in.vx[b]; vy = in.vy[b]; vz = in.vz[b];
   }
-#pragma unroll
-  for (int k = 0; k < 3; ++k) sp[k][tid] = p[k];
-  sv[tid] = b >= 0;
   if (tid < 3) med[tid] = 0.0;
   const int nv = __syncthreads_count(b >= 0);
-  if (b >= 0) {
+  if (tid < 32 && nv > 0) {
+    const int ns = min(32, nv);
+    // sample `tid` = slot tid * nv / 32 (all distinct when nv >= 32)
+    const int q = ns == 32 ? static_cast<int>((static_cast<long long>(tid) * nv) >> 5) : tid;
+    const int bq = q < ns || ns == 32 ? order[blockIdx.x * TJ + q] : -1;
+    double s[3] = {0.0, 0.0, 0.0};
+    if (tid < ns) {
+      s[0] = in.x[bq]; s[1] = in.y[bq]; s[2] = in.z[bq];
+    }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {  // rank of p[k] among the valid slots (ties by slot)
+    for (int k = 0; k < 3; ++k) {  // rank among the ns samples (ties by lane)
       int r = 0;
-      for (int q = 0; q < TJ; ++q) {
-        const double w = sp[k][q];
-        r += (sv[q] && (w < p[k] || (w == p[k] && q < tid))) ? 1 : 0;
+      for (int l = 0; l < ns; ++l) {
+        const double w = __shfl_sync(0xffffffffu, s[k], l);
+        r += (w < s[k] || (w == s[k] && l < tid)) ? 1 : 0;
       }
-      if (r == nv / 2) med[k] = p[k];
+      if (tid < ns && r == ns / 2) med[k] = s[k];
     }
   }
   __syncthreads();
