@@ -115,6 +115,19 @@ def test_dropin_row_range():
     assert np.all(empty == 0)
 
 
+def test_dropin_row_range_mixed():
+    """Tile-relative drop-in: a row range gives the full call's rows (the
+    j-records are the same; only the split of the j-sum may differ)."""
+    s = nb.plummer(3000, seed=4)
+    full = nb.force_calculation(s, eps2=1e-4, precision="mixed")
+    part = nb.force_calculation(s, eps2=1e-4, precision="mixed", i_begin=1000, i_end=2100)
+    assert np.all(part[:, :1000] == 0) and np.all(part[:, 2100:] == 0)
+    ea, ej = derivs_rel(part[:, 1000:2100], full[:, 1000:2100])
+    assert ea <= 1e-6 and ej <= 1e-5, (ea, ej)
+    ref = O.force(s, 1e-4)
+    assert vec_rel(full[:3], ref[:3]).max() <= 2e-4
+
+
 def test_fp64_deterministic():
     s = nb.plummer(5000, seed=9)
     a = engine_derivs(s, 1e-4)
