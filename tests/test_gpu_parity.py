@@ -154,10 +154,13 @@ def test_hermite_10_steps_vs_reference_golden(n):
     assert tm["steps"] == steps and abs(tm["t"] - steps * dt) < 1e-15
 
 
-def test_phase_calls_equal_graph_steps():
-    """prediction / eval / correction one at a time == the captured step graph."""
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_phase_calls_equal_graph_steps(precision):
+    """prediction / eval / correction one at a time == the captured step graph
+    (mixed: tile-relative, re-ordered every 2 steps on both paths)."""
     s = nb.plummer(1500, seed=4)
-    with nb.Engine(1500, eps2=1e-4, dt=1 / 1024) as a, nb.Engine(1500, eps2=1e-4, dt=1 / 1024) as b:
+    kw = dict(eps2=1e-4, dt=1 / 1024, precision=precision, sort_every=2)
+    with nb.Engine(1500, **kw) as a, nb.Engine(1500, **kw) as b:
         a.set_state(s)
         b.set_state(s)
         a.timestepping(5)
