@@ -163,14 +163,6 @@ __global__ void ens_key_kernel(int L, const int* __restrict__ cid, const int* __
   vals[r] = r;
 }
 
-// Sum of a row's split partials, field f.
-__device__ __forceinline__ double ens_split_sum(const double* __restrict__ P, const ClusterDev& k,
-                                                int f, int i) {
-  double v = 0.0;
-  for (int s = 0; s < k.S; ++s) v += P[k.p_off + (static_cast<long long>(s) * 6 + f) * k.ld + i];
-  return v;
-}
-
 __global__ void ens_correct_kernel(int L, const int* __restrict__ cid,
                                    const ClusterDev* __restrict__ cl, const double* __restrict__ P,
                                    double* __restrict__ X, double* __restrict__ V,
@@ -184,9 +176,11 @@ __global__ void ens_correct_kernel(int L, const int* __restrict__ cid,
   const double dt = k.dt;
   const double idt2 = 1.0 / (dt * dt), idt3 = idt2 / dt;
   const double dt3 = dt * dt * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
+  double sum[6];
+  split_sums(P + k.p_off, k.ld, k.S, i, sum);  // cluster partials: [S_c][6][ld_c]
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    const double a1 = ens_split_sum(P, k, q, i), j1 = ens_split_sum(P, k, 3 + q, i);
+    const double a1 = sum[q], j1 = sum[3 + q];
     const double a = D[q * L + r], j = D[(3 + q) * L + r];
     const double da = a - a1;
     const double a2 = 2.0 * idt2 * (-3.0 * da - (2.0 * j + j1) * dt);
@@ -206,7 +200,9 @@ __global__ void ens_reduce_kernel(int L, const int* __restrict__ cid,
   const int c = cid[r];
   if (c < 0) return;
   const ClusterDev k = cl[c];
-  for (int f = 0; f < 6; ++f) D[f * L + r] = ens_split_sum(P, k, f, r - k.row0);
+  double sum[6];
+  split_sums(P + k.p_off, k.ld, k.S, r - k.row0, sum);
+  for (int f = 0; f < 6; ++f) D[f * L + r] = sum[f];
 }
 
 // phi[r] = sum over the same cluster's j != r of m_j / sqrt(r^2 + eps2_c);

@@ -185,6 +185,22 @@ static __global__ void predict_kernel(int n, int ld, const StepCtl* __restrict__
   if (jbx2) jbx2[i] = make_jbx2(p[0], p[1], p[2], m, u[0], u[1], u[2]);
 }
 
+// sum[c] = sum over splits s = 0, 1, ..., S-1 (in that order) of
+// P[s][c][i], for the six fields at once: one pass over the splits with
+// several loads in flight, so a small system (few CTAs) is not bound by
+// one load latency per split.
+__device__ __forceinline__ void split_sums(const double* __restrict__ P, int ld, int S, int i,
+                                           double sum[6]) {
+#pragma unroll
+  for (int c = 0; c < 6; ++c) sum[c] = 0.0;
+#pragma unroll 4
+  for (int s = 0; s < S; ++s) {
+    const double* p = P + static_cast<size_t>(s) * 6 * ld + i;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) sum[c] += p[static_cast<size_t>(c) * ld];
+  }
+}
+
 // Corrector fused with the split-j reduction and the Aarseth criterion:
 // a1/j1 = sum over S splits of P; snap/crackle; correct X, V; D <- a1/j1.
 static __global__ void correct_kernel(int n, int ld, int S, const double* __restrict__ P,
@@ -199,13 +215,11 @@ static __global__ void correct_kernel(int n, int ld, int S, const double* __rest
     const double idt3 = idt2 / dt;
     const double dt3 = dt * dt * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
     double A2 = 0, J2 = 0, S2 = 0, C2 = 0;
+    double sum[6];
+    split_sums(P, ld, S, i, sum);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      double a1 = 0.0, j1 = 0.0;
-      for (int s = 0; s < S; ++s) {
-        a1 += P[(static_cast<size_t>(s) * 6 + c) * ld + i];
-        j1 += P[(static_cast<size_t>(s) * 6 + 3 + c) * ld + i];
-      }
+      const double a1 = sum[c], j1 = sum[3 + c];
       const double a = D[c * ld + i], j = D[(3 + c) * ld + i];
       const double da = a - a1;
       const double a2 = 2.0 * idt2 * (-3.0 * da - (2.0 * j + j1) * dt);
@@ -229,12 +243,10 @@ static __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int 
   const int i = i_begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= i_end) return;
   double* dst[6] = {out.ax, out.ay, out.az, out.jx, out.jy, out.jz};
+  double sum[6];
+  split_sums(P, ld, S, i, sum);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    double v = 0.0;
-    for (int s = 0; s < S; ++s) v += P[(static_cast<size_t>(s) * 6 + c) * ld + i];
-    dst[c][i] = v;
-  }
+  for (int c = 0; c < 6; ++c) dst[c][i] = sum[c];
 }
 
 // Initial step criterion min_i eta0 |a| / |j| (published via ctl).
