@@ -2,7 +2,8 @@
 //
 // j-body tiles move global -> shared with the non-tensor bulk copy
 // (cp.async.bulk ... mbarrier::complete_tx::bytes), issued by one thread and
-// tracked by an mbarrier transaction count.  No multicast form is used.
+// tracked by an mbarrier transaction count.  Every copy lands in the issuing
+// CTA's own shared memory and reads this GPU's own global memory.
 // Every wait is bounded by the global nanosecond timer: a wait that runs past
 // its limit reports failure instead of spinning forever.
 #pragma once
