@@ -230,6 +230,8 @@ __global__ void adj_post_kernel(int n, int ld, double h, double* __restrict__ AD
   } while (0)
 
 using FwdFP64 = RowsFP64<128, 2, kTile, 1>;
+using FwdFP64Small = RowsFP64<128, 1, kTile, 2>;  // n < kSmallN: twice the row blocks
+constexpr int kSmallN = 32768;
 using FwdMixed = RowsMixedX2<128, 4, kTile, 1, 1>;
 
 template <class R>
@@ -239,8 +241,8 @@ __global__ void __launch_bounds__(R::NT) adj_pair_kernel(const typename R::JB* _
   pair_system<R>(jb, a, smem_raw, full);
 }
 
-int splits_for(int sms, int row_blocks, int n_tiles) {
-  const int target = sms * 4;
+int splits_for(int sms, int row_blocks, int n_tiles, int ctas_per_sm) {
+  const int target = sms * ctas_per_sm;
   return std::max(1, std::min(n_tiles, (target + row_blocks - 1) / row_blocks));
 }
 
@@ -282,7 +284,11 @@ nbody_status fwd_eval(nbody_adjoint* a, cudaStream_t st) {
   pa.out = a->P;
   pa.stride = ld;
   pa.status = a->status;
-  if (fp64) {
+  if (fp64 && a->n < kSmallN) {
+    const dim3 grid((a->n + FwdFP64Small::ROWS - 1) / FwdFP64Small::ROWS, a->S);
+    adj_pair_kernel<FwdFP64Small><<<grid, FwdFP64Small::NT, pair_smem_bytes<FwdFP64Small>(), st>>>(
+        a->jb64, pa);
+  } else if (fp64) {
     const dim3 grid((a->n + FwdFP64::ROWS - 1) / FwdFP64::ROWS, a->S);
     adj_pair_kernel<FwdFP64><<<grid, FwdFP64::NT, pair_smem_bytes<FwdFP64>(), st>>>(a->jb64, pa);
   } else {
@@ -394,9 +400,13 @@ nbody_status nbody_adjoint_create(nbody_adjoint** out, const nbody_adjoint_confi
   a->ld = (cfg->n + kPad - 1) / kPad * kPad;
   a->nseg = std::max(1, (cfg->nsteps + cfg->checkpoint_every - 1) / cfg->checkpoint_every);
   cudaDeviceGetAttribute(&a->sms, cudaDevAttrMultiProcessorCount, cfg->device);
-  const int rows_fwd = cfg->precision == NBODY_FP64 ? FwdFP64::ROWS : FwdMixed::ROWS;
-  a->S = splits_for(a->sms, (a->n + rows_fwd - 1) / rows_fwd, a->ld / kTile);
-  a->Sv = splits_for(a->sms, (a->n + kVjpNT - 1) / kVjpNT, a->ld / kVjpTile);
+  const int rows_fwd = cfg->precision == NBODY_FP64
+                           ? (cfg->n < kSmallN ? FwdFP64Small::ROWS : FwdFP64::ROWS)
+                           : FwdMixed::ROWS;
+  // forward: small systems take as many j-splits as the wave allows (the
+  // pair pass is latency-bound there); VJP: about 4 CTAs per SM
+  a->S = splits_for(a->sms, (a->n + rows_fwd - 1) / rows_fwd, a->ld / kTile, 8);
+  a->Sv = splits_for(a->sms, (a->n + kVjpNT - 1) / kVjpNT, a->ld / kVjpTile, 4);
   nbody_adjoint* r = a.get();
   auto body = [&]() -> nbody_status {
     const size_t ld = r->ld;
@@ -425,6 +435,9 @@ nbody_status nbody_adjoint_create(nbody_adjoint** out, const nbody_adjoint_confi
     AD_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&adj_pair_kernel<FwdFP64>),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(pair_smem_bytes<FwdFP64>())));
+    AD_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&adj_pair_kernel<FwdFP64Small>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(pair_smem_bytes<FwdFP64Small>())));
     AD_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&vjp_pair_kernel),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(2 * kVjpTile * sizeof(JAdj))));

@@ -259,6 +259,10 @@ int choose_split(const nbody_engine* e, const PairKernel& k, int rows) {
   const long slots = static_cast<long>(e->num_sms) * occ;
   const long i_blocks = (rows + k.nt * k.ipt - 1) / (k.nt * k.ipt);
   const int n_tiles = e->ld / k.tj;
+  // A small system (a few tile-units of work per resident CTA slot) is
+  // latency-bound: the most CTAs win (N = 4096: S = 32 measured 40 us,
+  // S = 16 46 us, FP64 one row per thread).
+  if (i_blocks * n_tiles <= 4 * slots) return std::min(n_tiles, kMaxSplit);
   double best = 1e300;
   int best_s = 1;
   for (int s = 1; s <= std::min(kMaxSplit, n_tiles); ++s) {
@@ -399,10 +403,15 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
 // Tiling for `rows` i-rows: explicit config, else tuned, else heuristic.
 nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
   const nbody_config& c = e->cfg;
-  // defaults: the best measured shape of each family (Plummer N = 65536)
+  // defaults: the best measured shape of each family (Plummer N = 65536);
+  // small systems take half the rows per thread, which doubles their row
+  // blocks (FP64 below 32768 rows: N = 4096 40 vs 48 us per launch;
+  // tile-relative below 8192 rows)
   const bool rel = c.precision == NBODY_MIXED && c.pair_variant == 0;
   int nt = c.threads ? c.threads : 128;
-  int ipt = c.i_per_thread ? c.i_per_thread : (rel ? 4 : 2);
+  int ipt = c.i_per_thread ? c.i_per_thread
+                           : rel ? (rows < 8192 ? 2 : 4)
+                                 : (c.precision == NBODY_FP64 && rows < 32768 ? 1 : 2);
   int tj = c.j_tile ? c.j_tile : 128;
   const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, c.pair_variant);
   if (!k)
