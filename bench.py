@@ -345,6 +345,23 @@ def max_over_ranks_fn(world, dist, device):
     return f
 
 
+def arms_over_ranks(max_fn, main_arm, other):
+    """Slowest-rank step and pair times of both arms (other may be None).
+    Every rank calls this, with the same arms, in the same order."""
+    main_arm["ms_per_step"] = max_fn(main_arm["ms_per_step"])
+    main_arm["pair_ms"] = max_fn(main_arm["pair_ms"])
+    if other is not None:
+        other["ms_per_step"] = max_fn(other["ms_per_step"])
+        other["pair_ms"] = max_fn(other["pair_ms"])
+
+
+def e2e_over_ranks(max_fn, world, n, e2e):
+    """Whole-job e2e value from the slowest rank's drop-in call time."""
+    e2e["ms_per_call"] = max_fn(e2e["ms_per_call"])
+    e2e["value"] = world * float(n) * n / (e2e["ms_per_call"] * 1e-3) / 1e9
+    return e2e
+
+
 def replica_value(world, interactions_per_replica, ms_per_step):
     """Whole-job G interactions/s of `world` independent replicas timed at the
     slowest rank's step time."""
@@ -585,10 +602,14 @@ def main():
                                             "max": float(ea.max())},
                     "jerk_rel_err_vs_fp64": {"median": float(np.median(ej)), "p99": float(np.quantile(ej, 0.99)),
                                              "max": float(ej.max())}}
-    ms = max_over_ranks(main_arm["ms_per_step"])
-    pair_ms = max_over_ranks(main_arm["pair_ms"])
-    e2e = run_e2e(a, a.precision, state, torch, max(3, min(a.steps, 20)))
-    e2e["value"] = e2e["value"] * world
+    # every cross-rank reduction happens here, on all ranks, before the
+    # non-zero ranks leave
+    arms_over_ranks(max_over_ranks, main_arm, other)
+    ms, pair_ms = main_arm["ms_per_step"], main_arm["pair_ms"]
+    if world > 1:
+        dist.barrier()
+    e2e = e2e_over_ranks(max_over_ranks, world, a.n,
+                         run_e2e(a, a.precision, state, torch, max(3, min(a.steps, 20))))
     cpu = cpu_baseline(a, state) if (rank == 0 and world == 1 and not a.no_cpu_baseline) else None
     if world > 1:
         dist.barrier()
@@ -632,7 +653,7 @@ def main():
         "peaks_measured": peaks,
     }
     if other is not None:
-        ov = replica_value(world, inter, max_over_ranks(other["ms_per_step"]))
+        ov = replica_value(world, inter, other["ms_per_step"])
         line[other_prec] = {"value": ov, "ms_per_step": other["ms_per_step"], "pair_ms": other["pair_ms"],
                             "roofline": roofline(other, other_prec), "tiling": other["tiling"],
                             "clocks": other["clocks"]}

@@ -32,6 +32,42 @@ def _rank(rank, world, port, times, out):
     dist.destroy_process_group()
 
 
+def _rank_arms(rank, world, port, out):
+    """The bench's post-measurement reductions with rank-dependent timings;
+    rank 0 then leaves no collective pending (the others have returned)."""
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    mx = bench.max_over_ranks_fn(world, dist, "cpu")
+    main_arm = {"ms_per_step": 4.0 + rank, "pair_ms": 3.9 + rank}
+    other = {"ms_per_step": 8.0 + 2 * rank, "pair_ms": 7.9 + 2 * rank}
+    bench.arms_over_ranks(mx, main_arm, other)
+    dist.barrier()
+    e2e = bench.e2e_over_ranks(mx, world, 1000, {"ms_per_call": 5.0 + 0.5 * rank, "value": 0.0})
+    dist.barrier()
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+    out[0] = (main_arm, other, e2e)
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_post_measurement_reductions_gloo(world):
+    out = mp.Manager().dict()
+    mp.spawn(_rank_arms, args=(world, _free_port(), out), nprocs=world, join=True)
+    main_arm, other, e2e = out[0]
+    w = world - 1
+    assert main_arm == {"ms_per_step": 4.0 + w, "pair_ms": 3.9 + w}
+    assert other == {"ms_per_step": 8.0 + 2 * w, "pair_ms": 7.9 + 2 * w}
+    assert e2e["ms_per_call"] == 5.0 + 0.5 * w
+    assert abs(e2e["value"] - world * 1e6 / ((5.0 + 0.5 * w) * 1e-3) / 1e9) < 1e-12
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_replica_aggregation_gloo(world):
     times = [4.5 + 0.25 * r for r in range(world)]
