@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--tune", action="store_true", help="autotune pair-kernel tiling first")
     ap.add_argument("--variant", type=int, default=0,
-                    help="mixed pair kernel (nbody_config.pair_variant): 0 = tile-relative (default), "
-                         "1 = scalar hi/lo, 2/3 = packed hi/lo")
+                    help="mixed pair kernel (nbody_config.pair_variant): 0 = automatic (tile-relative "
+                         "from 8192 bodies), 1 = scalar hi/lo, 2/3 = packed hi/lo, 4 = tile-relative; "
+                         "ensembles: 3 = packed hi/lo, else tile-relative")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--kernels-only", action="store_true",
@@ -412,7 +413,7 @@ def main_ensemble(a):
     sizes, eps2, state = nb.plummer_ensemble(a.clusters, 3)
     dt = 1.0 / 512
     inter = float((sizes.astype(np.float64) ** 2).sum())
-    variant = a.variant if a.precision == "mixed" else 0
+    variant = 3 if a.precision == "mixed" and a.variant in (1, 2, 3) else 0
     ens = nb.Ensemble(sizes, eps2, dt, precision=a.precision, tune=True, pair_variant=variant)
     ens.set_state(state)
     ens.force_calculation()

@@ -65,16 +65,20 @@ typedef struct {
   double eta0;        /* initial-dt criterion, default 1e-4 (nbody.h:15)    */
   int tune;           /* 1: time candidate tilings on first use (autotuner) */
   int threads, i_per_thread, j_tile, split_j; /* 0 = choose automatically   */
-  int pair_variant;   /* mixed only: 0 = packed-pair (f32x2) kernel on
+  int pair_variant;   /* mixed only: 0 = automatic (variant 4 from 8192
+                         bodies, variant 3 below, where building the tiles
+                         costs more than it saves), 1 = scalar FP32 kernel
+                         on hi/lo positions, 2 = packed-pair (f32x2) hi/lo
+                         kernel, FP64 accumulators in registers, 3 = packed
+                         hi/lo kernel, FP64 accumulators in shared memory
+                         (the most accurate), 4 = packed-pair kernel on
                          tile-relative positions (Morton-ordered j-tiles,
-                         one add per separation component; the fastest),
-                         1 = scalar FP32 kernel on hi/lo positions,
-                         2 = packed-pair hi/lo kernel, FP64 accumulators in
-                         registers, 3 = packed-pair hi/lo kernel, FP64
-                         accumulators in shared memory (the most accurate) */
-  int sort_every;     /* variant 0: re-order the j-bodies along the Morton
-                         curve every this many steps (tile centres and
-                         offsets are rebuilt every step); 0 = 16          */
+                         one add per separation component; the fastest
+                         for large systems)                                 */
+  int sort_every;     /* tile-relative kernel: re-order the j-bodies along
+                         the Morton curve every this many steps (tile
+                         centres and offsets are rebuilt every step);
+                         0 = 16                                             */
 } nbody_config;
 
 typedef struct nbody_engine nbody_engine;

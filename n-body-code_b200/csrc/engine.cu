@@ -149,10 +149,10 @@ const std::vector<PairKernel>& registry() {
   return r;
 }
 
-// variant (mixed only): 0 = tile-relative packed pairs, 1 = scalar FP32
+// variant (mixed only, after resolving 0 = automatic): 1 = scalar FP32
 // hi/lo, 2 = packed hi/lo pairs with register accumulators, 3 = packed
 // hi/lo pairs with shared-memory FP64 accumulators (falling back to
-// register accumulators where that shape has none).
+// register accumulators where that shape has none), 4 = tile-relative.
 const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
   auto match = [&](int fmt, int acc) -> const PairKernel* {
     for (const auto& k : registry())
@@ -163,14 +163,12 @@ const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int varian
   };
   if (precision == NBODY_FP64) return match(kRecF64, -1);
   if (variant == 1) return match(kRecF32, -1);
-  if (variant == 0) return match(kRecRel, -1);
+  if (variant == 4) return match(kRecRel, -1);
   if (variant == 2) return match(kRecX2, 0);
   const PairKernel* k = match(kRecX2, 1);
   return k ? k : match(kRecX2, 0);
 }
 
-// Record format of a precision's variant-0 kernels (the autotuner's family).
-int default_format(int precision) { return precision == NBODY_FP64 ? kRecF64 : kRecRel; }
 
 struct Tiling {
   const PairKernel* k = nullptr;
@@ -220,6 +218,10 @@ struct nbody_engine {
   bool tiled = false;
   cudaGraphExec_t graph = nullptr;
   int graph_kernels = 0;  // kernel nodes of the captured step
+  // automatic mixed kernel (pair_variant 0): tile-relative from this many
+  // bodies, packed hi/lo below.  Engines re-order every sort_every steps;
+  // the drop-in re-orders on every call and raises the threshold.
+  int rel_min_bodies = 8192;
   cudaGraphExec_t order_graph = nullptr;  // captured Morton re-ordering (variant 0)
   cudaStream_t aux = nullptr;              // drop-in: uploads that overlap the ordering
   cudaEvent_t aux_ev[2] = {nullptr, nullptr};
@@ -234,6 +236,20 @@ struct nbody_engine {
 namespace {
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// The mixed kernel family in use: pair_variant, with 0 (automatic)
+// resolved by the system size.
+int effective_variant(const nbody_engine* e) {
+  const nbody_config& c = e->cfg;
+  if (c.precision != NBODY_MIXED || c.pair_variant != 0) return c.pair_variant;
+  return e->n >= e->rel_min_bodies ? 4 : 3;
+}
+
+// Record format of the autotuner's family (the automatic choice).
+int default_format(const nbody_engine* e) {
+  if (e->cfg.precision == NBODY_FP64) return kRecF64;
+  return effective_variant(e) == 4 ? kRecRel : kRecX2;
+}
 
 nbody_status check_status_word(nbody_engine* e) {
   int h = 0;
@@ -366,7 +382,7 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   const auto& reg = registry();
   for (size_t idx = 0; idx < reg.size(); ++idx) {
     const PairKernel& k = reg[idx];
-    if (k.precision != e->cfg.precision || k.fmt != default_format(k.precision)) continue;
+    if (k.precision != e->cfg.precision || k.fmt != default_format(e)) continue;
     const int s0 = choose_split(e, k, rows);
     NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt, k.tj));
     for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
@@ -407,17 +423,18 @@ nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
   // small systems take half the rows per thread, which doubles their row
   // blocks (FP64 below 32768 rows: N = 4096 40 vs 48 us per launch;
   // tile-relative below 8192 rows)
-  const bool rel = c.precision == NBODY_MIXED && c.pair_variant == 0;
+  const int variant = effective_variant(e);
+  const bool rel = c.precision == NBODY_MIXED && variant == 4;
   int nt = c.threads ? c.threads : 128;
   int ipt = c.i_per_thread ? c.i_per_thread
                            : rel ? (rows < 8192 ? 2 : 4)
                                  : (c.precision == NBODY_FP64 && rows < 32768 ? 1 : 2);
   int tj = c.j_tile ? c.j_tile : 128;
-  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, c.pair_variant);
+  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, variant);
   if (!k)
     return fail(NBODY_ERR_INVALID_ARG,
                 "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d variant=%d", nt,
-                ipt, tj, c.pair_variant);
+                ipt, tj, variant);
   if (c.tune && !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j && !c.pair_variant)
     return autotune(e, rows, out);
   out->k = k;
@@ -693,7 +710,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
   if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
-  if (cfg->pair_variant < 0 || cfg->pair_variant > 3)
+  if (cfg->pair_variant < 0 || cfg->pair_variant > 4)
     return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
   if (cfg->sort_every < 0) return fail(NBODY_ERR_INVALID_ARG, "sort_every = %d", cfg->sort_every);
   int ndev = 0;
@@ -1033,6 +1050,9 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     c.device = dev;
     c.dt = 1.0;  // fixed: no initial-dt pass on the drop-in path
     NB_TRY(nbody_create(&d.e, &c));
+    // every call re-orders: tile-relative pays off only above ~24k bodies
+    // (measured per call: N = 16384 428 vs 357 us hi/lo; N = 65536 it wins)
+    d.e->rel_min_bodies = 32768;
     d.n = n;
     d.eps2 = eps2;
   }

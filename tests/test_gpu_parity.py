@@ -83,15 +83,18 @@ def test_fp64_every_tiling_agrees(tiling):
     dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
     dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1),
     dict(threads=128, i_per_thread=4, j_tile=128, split_j=9, pair_variant=2),
-    # tile-relative (0, the default)
-    dict(threads=128, i_per_thread=4, j_tile=128, split_j=1),
-    dict(threads=128, i_per_thread=2, j_tile=128, split_j=7),
-    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64),
-    dict(threads=256, i_per_thread=2, j_tile=128, split_j=3),
-    dict(threads=256, i_per_thread=4, j_tile=128, split_j=2),
-    dict(threads=128, i_per_thread=2, j_tile=64, split_j=5),
-    dict(threads=128, i_per_thread=4, j_tile=64, split_j=2),
-    dict(threads=128, i_per_thread=2, j_tile=256, split_j=2)])
+    # tile-relative (4; the automatic choice from 8192 bodies)
+    dict(threads=128, i_per_thread=4, j_tile=128, split_j=1, pair_variant=4),
+    dict(threads=128, i_per_thread=2, j_tile=128, split_j=7, pair_variant=4),
+    dict(threads=64, i_per_thread=4, j_tile=128, split_j=64, pair_variant=4),
+    dict(threads=256, i_per_thread=2, j_tile=128, split_j=3, pair_variant=4),
+    dict(threads=256, i_per_thread=4, j_tile=128, split_j=2, pair_variant=4),
+    dict(threads=128, i_per_thread=2, j_tile=64, split_j=5, pair_variant=4),
+    dict(threads=128, i_per_thread=4, j_tile=64, split_j=2, pair_variant=4),
+    dict(threads=128, i_per_thread=2, j_tile=256, split_j=2, pair_variant=4),
+    # automatic (0): packed hi/lo at this size
+    dict(),
+    dict(split_j=3)])
 def test_mixed_every_kernel_agrees(tiling):
     """Tile-relative, packed hi/lo and scalar mixed kernels, every shape:
     same accuracy class."""
@@ -115,17 +118,20 @@ def test_dropin_row_range():
     assert np.all(empty == 0)
 
 
-def test_dropin_row_range_mixed():
-    """Tile-relative drop-in: a row range gives the full call's rows (the
-    j-records are the same; only the split of the j-sum may differ)."""
-    s = nb.plummer(3000, seed=4)
+@pytest.mark.parametrize("n", [3000, 40000])
+def test_dropin_row_range_mixed(n):
+    """Mixed drop-in (packed hi/lo at 3000 bodies, tile-relative at 40000): a
+    row range gives the full call's rows (the j-records are the same; only
+    the split of the j-sum may differ)."""
+    s = nb.plummer(n, seed=4)
     full = nb.force_calculation(s, eps2=1e-4, precision="mixed")
     part = nb.force_calculation(s, eps2=1e-4, precision="mixed", i_begin=1000, i_end=2100)
     assert np.all(part[:, :1000] == 0) and np.all(part[:, 2100:] == 0)
     ea, ej = derivs_rel(part[:, 1000:2100], full[:, 1000:2100])
     assert ea <= 1e-6 and ej <= 1e-5, (ea, ej)
-    ref = O.force(s, 1e-4)
-    assert vec_rel(full[:3], ref[:3]).max() <= 2e-4
+    rows = np.arange(0, n, max(1, n // 300))
+    ref = O.force_rows(s, 1e-4, rows)
+    assert vec_rel(full[:3, rows], ref[:3]).max() <= 2e-4
 
 
 def test_fp64_deterministic():
@@ -154,12 +160,12 @@ def test_hermite_10_steps_vs_reference_golden(n):
     assert tm["steps"] == steps and abs(tm["t"] - steps * dt) < 1e-15
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_phase_calls_equal_graph_steps(precision):
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("mixed", 3), ("mixed", 4)])
+def test_phase_calls_equal_graph_steps(precision, variant):
     """prediction / eval / correction one at a time == the captured step graph
-    (mixed: tile-relative, re-ordered every 2 steps on both paths)."""
+    (tile-relative: re-ordered every 2 steps on both paths)."""
     s = nb.plummer(1500, seed=4)
-    kw = dict(eps2=1e-4, dt=1 / 1024, precision=precision, sort_every=2)
+    kw = dict(eps2=1e-4, dt=1 / 1024, precision=precision, sort_every=2, pair_variant=variant)
     with nb.Engine(1500, **kw) as a, nb.Engine(1500, **kw) as b:
         a.set_state(s)
         b.set_state(s)
@@ -289,10 +295,11 @@ def test_max_size_sampled_rows(precision):
 
 
 # ---------------------------------------------------------------------------
-# Tile-relative mixed kernel (pair_variant 0, the default): j-bodies in
-# Morton-ordered tiles, positions as float offsets from the tile centre.
+# Tile-relative mixed kernel (pair_variant 4; the automatic choice from 8192
+# bodies): j-bodies in Morton-ordered tiles, positions as float offsets from
+# the tile centre.
 # ---------------------------------------------------------------------------
-REL = dict(pair_variant=0)
+REL = dict(pair_variant=4)
 HILO = dict(pair_variant=3)
 
 
