@@ -159,7 +159,9 @@ const char* nbody_status_string(nbody_status s);
  * the range stay zero, so an MPI caller that sums ranks (src/nbody.cpp:
  * 240-246) gets the complete result.  A cached engine per (thread, device)
  * is reused, so repeated calls allocate nothing after the first.  Copies
- * host->device and back inside the call (the reference contract). */
+ * host->device and back inside the call (the reference contract).
+ * precision = NBODY_MIXED: the tile-relative kernel from 32768 bodies (each
+ * call re-orders the bodies), the packed hi/lo kernel below. */
 nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin, int i_end,
                                      const double* x, const double* y, const double* z,
                                      const double* m, const double* vx, const double* vy,
