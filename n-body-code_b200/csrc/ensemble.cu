@@ -359,7 +359,9 @@ nbody_status build_items(nbody_ensemble* e, int tpi) {
   std::vector<EnsItem> items;
   long long p_off = 0;
   for (int c = 0; c < e->C; ++c) {
-    const int tiles = e->ld[c] / e->kern->tile;
+    // j-tiles that hold bodies: the padding rows of a segment come last (in
+    // the tile-relative order too), so whole padding tiles are skipped
+    const int tiles = (e->n[c] + e->kern->tile - 1) / e->kern->tile;
     const int S = (tiles + tpi - 1) / tpi;
     cl[c] = ClusterDev{e->row0[c], e->n[c], e->ld[c], S, p_off, e->eps2[c], e->dt[c]};
     for (int rb = 0; rb < e->ld[c] / kPadRows; ++rb)
