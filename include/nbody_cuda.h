@@ -57,7 +57,7 @@ typedef struct {
   int n;              /* bodies, >= 1                                       */
   double eps2;        /* softening^2, 1e-30 <= eps2 <= 1e30 (runtime; the
                          reference hard-codes 1e-7: include/kernel.h:13)    */
-  int precision;      /* nbody_precision                                    */
+  int precision;      /* nbody_precision (mixed: eps2 >= 1e-24)             */
   int device;         /* CUDA ordinal                                       */
   double dt;          /* > 0: fixed shared step; <= 0: adaptive (Aarseth,
                          src/nbody.cpp:131-150, 198-222)                    */

@@ -387,6 +387,9 @@ nbody_status nbody_adjoint_create(nbody_adjoint** out, const nbody_adjoint_confi
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "nsteps = %d, checkpoint_every = %d", cfg->nsteps, cfg->checkpoint_every);
   if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
+  if (cfg->precision == NBODY_MIXED && cfg->eps2 < kMinEps2Mixed)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG, "eps2 = %g below %g (mixed precision)", cfg->eps2,
+                           kMinEps2Mixed);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return nbody_set_error(NBODY_ERR_NO_DEVICE, "no CUDA device");
   if (cfg->device < 0 || cfg->device >= ndev) return nbody_set_error(NBODY_ERR_INVALID_ARG, "device %d", cfg->device);

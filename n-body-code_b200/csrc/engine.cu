@@ -705,6 +705,10 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (cfg->n < 1 || cfg->n > (1 << 28)) return fail(NBODY_ERR_INVALID_ARG, "n = %d out of range", cfg->n);
   if (!(cfg->eps2 >= 1e-30 && cfg->eps2 <= 1e30))
     return fail(NBODY_ERR_INVALID_ARG, "eps2 = %g outside [1e-30, 1e30]", cfg->eps2);
+  if (cfg->precision == NBODY_MIXED && cfg->eps2 < kMinEps2Mixed)
+    return fail(NBODY_ERR_INVALID_ARG,
+                "eps2 = %g below %g: the mixed path's float self-pair factor would overflow",
+                cfg->eps2, kMinEps2Mixed);
   if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
     return fail(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");

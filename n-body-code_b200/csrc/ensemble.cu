@@ -634,6 +634,9 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     if (cfg->n[c] < 1) return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d has n = %d", c, cfg->n[c]);
     if (!(cfg->eps2[c] >= 1e-30 && cfg->eps2[c] <= 1e30))
       return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d eps2 = %g", c, cfg->eps2[c]);
+    if (cfg->precision == NBODY_MIXED && cfg->eps2[c] < kMinEps2Mixed)
+      return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d eps2 = %g below %g (mixed precision)",
+                             c, cfg->eps2[c], kMinEps2Mixed);
     if (!(cfg->dt[c] > 0)) return nbody_set_error(NBODY_ERR_INVALID_ARG, "cluster %d dt = %g (ensembles use fixed steps)", c, cfg->dt[c]);
     L += (cfg->n[c] + kPadRows - 1) / kPadRows * kPadRows;
   }

@@ -107,6 +107,10 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "nbody_acc_jerk_noalloc: eps2 = %g outside [1e-30, 1e30]", eps2);
   if (precision != NBODY_FP64 && precision != NBODY_MIXED)
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "nbody_acc_jerk_noalloc: precision = %d", precision);
+  if (precision == NBODY_MIXED && eps2 < kMinEps2Mixed)
+    return nbody_set_error(NBODY_ERR_INVALID_ARG,
+                           "nbody_acc_jerk_noalloc: eps2 = %g below %g (mixed precision)", eps2,
+                           kMinEps2Mixed);
   const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
   for (const void* p : ptrs)
     if (!p) return nbody_set_error(NBODY_ERR_INVALID_ARG, "nbody_acc_jerk_noalloc: null array");

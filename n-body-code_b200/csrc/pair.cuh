@@ -39,6 +39,11 @@
 
 namespace nbody {
 
+// Smallest softening the FP32 pair math accepts: every row's self pair is
+// evaluated (r = 0, s = eps2) and its factor m s^(-3/2) must stay finite in
+// float (1e36 x m here; 3.4e38 is the float limit), else 0 x inf = NaN.
+constexpr double kMinEps2Mixed = 1e-24;
+
 // j-record, FP64 path: 64 bytes.
 struct __align__(16) JBody64 {
   double x, y, z, m, vx, vy, vz, pad;

@@ -393,3 +393,17 @@ def test_tile_relative_device_entry_and_steps():
     for name in ("rel1", "rel16"):
         dx = max(np.abs(runs[name][k] - runs["fp64"][k]).max() for k in ("x", "y", "z"))
         assert dx <= 1e-8, (name, dx)
+
+
+def test_mixed_rejects_softening_too_small_for_float():
+    """m eps2^-1.5 overflows float below eps2 ~ 1e-25 (the self pair would
+    give 0 x inf = NaN): mixed engines refuse eps2 < 1e-24, FP64 accepts it."""
+    with pytest.raises(nb.NBodyError, match="mixed"):
+        nb.Engine(64, eps2=1e-26, precision="mixed", dt=1.0)
+    s = nb.plummer(64, seed=1)
+    d = engine_derivs(s, 1e-26)
+    assert np.all(np.isfinite(d))
+    with nb.Engine(64, eps2=1e-24, precision="mixed", dt=1.0) as e:
+        e.set_state(s)
+        e.force_calculation()
+        assert np.all(np.isfinite(e.get_derivs()))

@@ -34,6 +34,9 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     msg = nb.load().nbody_last_error().decode()
     assert "32768" in msg and "scratch" in msg
     assert f(0, 1e-4, 0, *([z] * 13), None) == 1
+    # mixed precision: the float self-pair factor m eps2^-1.5 must stay finite
+    assert f(100, 1e-26, 1, *([z] * 13), None) == 1
+    assert "mixed" in nb.load().nbody_last_error().decode()
 
 
 @pytest.mark.gpu
