@@ -288,6 +288,8 @@ const std::vector<EnsKernel>& ens_registry() {
       ens_kernel_rel<RowsMixedRel<128, 2, 128, 1, 1>>(),
       ens_kernel_rel<RowsMixedRel<128, 2, 64, 1, 1>>(),
       ens_kernel_rel<RowsMixedRel<64, 4, 64, 1, 2>>(),
+      ens_kernel_rel<RowsMixedRel<128, 2, 128, 1, 2>>(),
+      ens_kernel_rel<RowsMixedRel<64, 4, 128, 1, 2>>(),
       ens_kernel<RowsMixedX2<64, 4, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<128, 2, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<64, 4, 64, 1, 1>>(NBODY_MIXED),
