@@ -309,7 +309,7 @@ nbody_status nbody_plummer(int n, uint64_t seed, double* x, double* y, double* z
                            double* vx, double* vy, double* vz);
 /* The reference's own initial conditions (src/nbody.cpp:69-114: std::mt19937
  * seed 42, vmax = rmax = mmax = 1, mmin = 0.01, virial rescale with the
- * reference potential at eps2) - the config-1 bodies. */
+ * reference potential at eps2) - the bodies of its `--N 1024` default run. */
 nbody_status nbody_reference_ic(int n, double eps2, double* x, double* y, double* z, double* m,
                                 double* vx, double* vy, double* vz);
 

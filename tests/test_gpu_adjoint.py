@@ -72,7 +72,7 @@ def test_gradient_vs_tangent_linear(nsteps, k):
         assert abs(g - dL) <= 1e-9 * abs(dL), (trial, g, dL)
 
 
-def test_config5_gradients_vs_finite_differences():
+def test_n4096_256_step_gradients_vs_finite_differences():
     """N = 4096 Plummer (seed 4), eps = 1e-2, dt = 1/256, 256 steps,
     checkpoint every 16; loss over 64 seeded bodies with targets = final
     positions + N(0, 1e-3).  FP64 central differences on sampled components."""

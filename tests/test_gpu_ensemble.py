@@ -99,7 +99,7 @@ def test_ensemble_deterministic(small_ensemble):
 
 
 def test_plummer_ensemble_config():
-    """Config-4-like clusters: the mixed path's energy error stays within 2x
+    """Plummer clusters with N log-uniform in [256, 8192]: the mixed path's energy error stays within 2x
     of the FP64 path's on the same run (at eps = 4/N and dt = 1/512 the
     integration error itself is large for the biggest clusters)."""
     sizes, eps2, state = nb.plummer_ensemble(64, seed=3)
