@@ -12,6 +12,7 @@
 //                                  (default for reference ICs) or m_i m_j
 //   --load <file> / --dump <file>  state files (nbody_read/write_state_file)
 //   --device <d> --tune
+//   --pair-variant <v>     mixed kernel: 0 automatic, 1-3 hi/lo forms, 4 tile-relative
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -39,7 +40,7 @@ int usage(const std::string& arg) {
   std::cerr << "Usage: ./nbody_app [--N <value>] [--Ncycle <value>] [--eps <e>] [--dt <h>] "
                "[--precision fp64|mixed] [--ic reference|plummer] [--seed <s>] "
                "[--energy reference|physical] [--load <file>] [--dump <file>] [--device <d>] "
-               "[--tune]"
+               "[--tune] [--pair-variant <v>]"
             << std::endl;
   return 1;
 }
@@ -86,6 +87,8 @@ int main(int argc, char* argv[]) {
         opt.device = std::stoi(argv[++i]);
       } else if (arg == "--tune") {
         opt.tune = true;
+      } else if (arg == "--pair-variant" && has) {
+        opt.pair_variant = std::stoi(argv[++i]);
       } else {
         return usage(arg);
       }

@@ -28,6 +28,7 @@ NBody::NBody(int Nparticles, double v_max, double r_max, double m_min, double m_
   c.device = opt.device;
   c.dt = opt.fixed_dt;
   c.tune = opt.tune ? 1 : 0;
+  c.pair_variant = opt.pair_variant;
   check(nbody_create(&eng_, &c), "nbody_create");
   nbody_timers t;
   check(nbody_get_timers(eng_, &t), "nbody_get_timers");

@@ -43,6 +43,7 @@ struct Options {
   bool reference_energy = true;  // the reference's printed potential (m_j^2 term)
   int device = 0;
   bool tune = false;
+  int pair_variant = 0;        // mixed kernel (nbody_config.pair_variant; 0 = automatic)
   std::string load_path;       // start from a state file instead of fresh ICs
 };
 

@@ -54,3 +54,14 @@ def test_fixed_dt_plummer_and_state_files(tmp_path):
     sys.path.insert(0, os.path.join(ROOT, "n-body-code_b200"))
     hdr = np.fromfile(b, dtype=np.float64, count=8)
     assert abs(hdr[2] - 36 / 1024) < 1e-12   # model time continued across the restart
+
+
+@pytest.mark.parametrize("variant", [3, 4])
+def test_mixed_kernel_choice_from_the_cli(variant):
+    """--pair-variant selects the mixed kernel (3 packed hi/lo, 4 tile-relative):
+    both keep the fixed-dt energy error of a short Plummer run small."""
+    vals, rows, _ = run("--N", 8192, "--Ncycle", 8, "--ic", "plummer", "--seed", 2, "--eps", 0.01,
+                        "--dt", 1 / 1024, "--precision", "mixed", "--pair-variant", variant,
+                        "--energy", "physical")
+    assert len(rows) == 8
+    assert vals["Err"] < 1e-7, vals
