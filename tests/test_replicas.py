@@ -85,3 +85,21 @@ def test_single_rank_is_identity():
     import bench
     assert bench.max_over_ranks_fn(1, None, "cpu")(3.25) == 3.25
     assert bench.replica_value(1, 1e9, 1000.0) == 1.0
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_ensemble_cluster_shards(world):
+    """bench.py --ensemble under torchrun shares the clusters out over the
+    GPUs: every cluster on exactly one rank, the same assignment on every
+    rank, per-rank work (sum of N^2) within one cluster's work of each other."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    rng = np.random.default_rng(3)
+    sizes = np.exp(rng.uniform(np.log(256), np.log(8192), 512)).astype(np.int32)
+    shards = [bench.shard_clusters(sizes, world, r) for r in range(world)]
+    allc = np.sort(np.concatenate(shards))
+    assert np.array_equal(allc, np.arange(sizes.size))
+    assert all(np.array_equal(s, bench.shard_clusters(sizes, world, r)) for r, s in enumerate(shards))
+    load = [float((sizes[s].astype(np.float64) ** 2).sum()) for s in shards]
+    assert max(load) - min(load) <= float(sizes.max()) ** 2
