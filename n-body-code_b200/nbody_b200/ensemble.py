@@ -48,7 +48,10 @@ def _f(name):
 
 
 class Ensemble:
-    """Clusters of sizes n[c] with softening eps2[c] and fixed step dt[c]."""
+    """Clusters of sizes n[c] with softening eps2[c] and fixed step dt[c].
+
+    Mixed precision: pair_variant 0 (default) uses tile-relative records, each
+    cluster Morton-ordered in its own segment; 3 uses the packed hi/lo kernel."""
 
     def __init__(self, n, eps2, dt, precision: str = "mixed", device: int = 0,
                  tiles_per_item: int = 0, tune: bool = False, pair_variant: int = 0,
