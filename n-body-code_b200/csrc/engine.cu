@@ -52,6 +52,7 @@ constexpr int kMaxSplit = 64;    // split-j upper bound
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
 constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
 constexpr int kMortonBits = 48;     // Morton key width (morton_key_kernel)
+constexpr int kMaxPotSplit = 32;    // j-splits of the potential diagnostic
 
 thread_local std::string g_last_error;
 
@@ -762,7 +763,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
       NB_CUDA(cudaMalloc(&e->sort_tmp, std::max<size_t>(e->sort_tmp_bytes, 16)));
     }
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
-    NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 + 8)));
+    NB_CUDA(cudaMalloc(&e->partial, sizeof(double) * (ld / kBlockO1 * kMaxPotSplit + 8)));
     NB_CUDA(cudaMalloc(&e->status, sizeof(int)));
     NB_CUDA(cudaMemsetAsync(e->status, 0, sizeof(int), e->stream));
     NB_CUDA(cudaStreamSynchronize(e->stream));
@@ -906,13 +907,15 @@ nbody_status nbody_energy(nbody_engine* e, int ref_compat, double* T, double* U)
   TraceRange trace_("nbody_energy");
   NB_TRY(need_state(e));
   const int nb = e->ld / kBlockO1;
-  double* scal = e->partial + nb;  // two result slots after the partials
+  // j-splits of the potential: about 8 CTAs per SM in all
+  const int ps = std::max(1, std::min({kMaxPotSplit, nb, (8 * e->num_sms + nb - 1) / nb}));
+  double* scal = e->partial + nb * kMaxPotSplit;  // two result slots after the partials
   kinetic_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->V, e->M, e->partial);
   sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal);
   pack_kernel<<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, own_inputs(e), e->jbe, nullptr, nullptr);
-  potential_kernel<kBlockO1><<<nb, kBlockO1, 0, e->stream>>>(e->n, e->ld, e->cfg.eps2,
-                                                             ref_compat ? 1 : 0, e->jbe, e->partial);
-  sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb, e->partial, scal + 1);
+  potential_kernel<kBlockO1><<<dim3(nb, ps), kBlockO1, 0, e->stream>>>(
+      e->n, e->ld, e->cfg.eps2, ref_compat ? 1 : 0, e->jbe, e->partial);
+  sum_partials_kernel<<<1, 256, 0, e->stream>>>(nb * ps, e->partial, scal + 1);
   NB_CUDA(cudaGetLastError());
   double h[2];
   NB_CUDA(cudaMemcpyAsync(h, scal, sizeof h, cudaMemcpyDeviceToHost, e->stream));

@@ -281,7 +281,10 @@ static __global__ void kinetic_kernel(int n, int ld, const double* __restrict__ 
 // (mode 0; CTA partial of m_i phi_i) or psi_i = sum_{j < i} 1/sqrt(.)
 // (mode 1, the reference's printed potential sum_i sum_{j>i} m_j^2/r_ij
 // regrouped by j; CTA partial of m_i^2 psi_i).  FP64, j-tiles staged
-// through shared memory by the CTA's threads.
+// through shared memory by the CTA's threads.  The j-range is split over
+// gridDim.y (CTA (x, y) takes tiles [y*tps, (y+1)*tps)), so a system of few
+// row blocks still fills the GPU; partial[y*gridDim.x + x] holds each CTA's
+// sum and sum_partials_kernel adds them in that fixed order.
 template <int NT>
 static __global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, double eps2, int mode,
                                                        const JBody64* __restrict__ jb,
@@ -290,8 +293,12 @@ static __global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, dou
   __shared__ double sh[32];
   const int i = blockIdx.x * NT + threadIdx.x;
   const JBody64 bi = jb[min(i, ld - 1)];
-  double phi = 0.0;
-  for (int j0 = 0; j0 < ld; j0 += NT) {
+  const int tiles = ld / NT, tps = (tiles + gridDim.y - 1) / gridDim.y;
+  const int jb0 = blockIdx.y * tps * NT, jb1 = min(ld, (blockIdx.y + 1) * tps * NT);
+  // four accumulators (partner k adds into acc[k % 4]), combined in a fixed
+  // order: four independent add chains instead of one
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j0 = jb0; j0 < jb1; j0 += NT) {
     const JBody64 bj = jb[j0 + threadIdx.x];
     tile[threadIdx.x] = make_double4(bj.x, bj.y, bj.z, bj.m);
     __syncthreads();
@@ -302,14 +309,15 @@ static __global__ void __launch_bounds__(NT) potential_kernel(int n, int ld, dou
       const double dx = p.x - bi.x, dy = p.y - bi.y, dz = p.z - bi.z;
       const double y = rsqrt_f64(fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2))));
       const bool take = mode == 0 ? (j != i) : (j < i);
-      phi += take ? (mode == 0 ? p.w * y : y) : 0.0;
+      acc[k & 3] += take ? (mode == 0 ? p.w * y : y) : 0.0;
     }
     __syncthreads();
   }
+  const double phi = (acc[0] + acc[1]) + (acc[2] + acc[3]);
   double e = 0.0;
   if (i < n) e = mode == 0 ? bi.m * phi : bi.m * bi.m * phi;
   const double b = block_sum(e, sh);
-  if (threadIdx.x == 0) partial[blockIdx.x] = b;
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = b;
 }
 
 // Sums `count` partials in a fixed order (one CTA).
