@@ -30,6 +30,7 @@
 //   orc_hermite_fixed     src/nbody.cpp:224-289   timestepping without updatedt
 // New (no reference counterpart), used as checkers for the GPU engine:
 //   orc_force_rows_fp64   direct j-sum for selected i-rows (large-N sampling)
+//   orc_force_rows_f32    the same with the _F32 pair arithmetic
 //   orc_potential_rows    per-row potential phi_i = -sum_{j!=i} m_j/r_ij
 //   orc_force_jvp         tangent (forward-mode derivative) of the pair
 //                         acc/jerk along a direction (dx, dv, dm)
@@ -187,6 +188,50 @@ void orc_force_rows_fp64(int n, double eps2, const double* x, const double* y, c
       j0 += w * (ux + c * rx);
       j1 += w * (uy + c * ry);
       j2 += w * (uz + c * rz);
+    }
+    out[0 * nrows + k] = a0;
+    out[1 * nrows + k] = a1;
+    out[2 * nrows + k] = a2;
+    out[3 * nrows + k] = j0;
+    out[4 * nrows + k] = j1;
+    out[5 * nrows + k] = j2;
+  }
+}
+
+// The _F32 pair arithmetic of orc_force_f32 (src/kernel.cpp:1101-1163) as a
+// direct sum over all j != i for a list of i-rows: every pair's float terms
+// are those the symmetric loop produces for that row (negating both
+// separations leaves each rounded float product and sum negated exactly), only
+// the order of the double accumulation differs.  The large-N accuracy floor
+// of the mixed kernels.  out is [6][nrows].
+void orc_force_rows_f32(int n, double eps2, const double* x, const double* y, const double* z,
+                        const double* m, const double* vx, const double* vy, const double* vz,
+                        int nrows, const int* rows, double* out) {
+  for (int k = 0; k < nrows; ++k) {
+    const int i = rows[k];
+    double a0 = 0, a1 = 0, a2 = 0, j0 = 0, j1 = 0, j2 = 0;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const float rx = (float)(x[j] - x[i]);
+      const float ry = (float)(y[j] - y[i]);
+      const float rz = (float)(z[j] - z[i]);
+      const float ux = (float)(vx[j] - vx[i]);
+      const float uy = (float)(vy[j] - vy[i]);
+      const float uz = (float)(vz[j] - vz[i]);
+      const float r2f = rx * rx + ry * ry + rz * rz;
+      const float s = (float)((double)r2f + eps2);
+      const float rv = rx * ux + ry * uy + rz * uz;
+      const float inv = (float)orc_invsqrt2d((double)s);
+      const float inv2 = inv * inv;
+      const float q = inv2 * inv;
+      const float c = (float)((-3.0 * (double)rv) * (double)inv2);
+      const float wj = (float)(m[j] * (double)q);
+      a0 += (double)(rx * wj);
+      a1 += (double)(ry * wj);
+      a2 += (double)(rz * wj);
+      j0 += (double)(wj * (ux + c * rx));
+      j1 += (double)(wj * (uy + c * ry));
+      j2 += (double)(wj * (uz + c * rz));
     }
     out[0 * nrows + k] = a0;
     out[1 * nrows + k] = a1;

@@ -35,17 +35,18 @@ _lib = None
 _ref = {}
 
 
-def build(with_reference: bool | None = None) -> None:
-    """Compile the restatement (always) and the reference build (when the
-    reference tree is present)."""
-    ref_tree = os.environ.get("NBODY_REFERENCE_TREE", "/root/reference")
+def build(ref_tree: str | None = None) -> None:
+    """Compile the restatement (always) and, given the reference tree
+    (`ref_tree`, else the NBODY_REFERENCE_TREE environment variable; there is
+    no default location), the reference build in oracle/_ref."""
+    ref_tree = ref_tree or os.environ.get("NBODY_REFERENCE_TREE")
     targets = ["oracle"]
-    if with_reference or (with_reference is None and os.path.isdir(ref_tree)):
+    if ref_tree and os.path.isdir(ref_tree):
         targets.append("ref")
         # the reference's own driver linked against the engine library
         if os.path.exists(os.path.join(HERE, "..", "n-body-code_b200", "lib", "libnbody_cuda.so")):
             targets.append("ref_gpu")
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_tree}", *targets], check=True,
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_tree or ''}", *targets], check=True,
                    stdout=subprocess.DEVNULL)
 
 
@@ -58,12 +59,13 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(_LIB):
-            build(with_reference=False)
+            build()
         L = C.CDLL(_LIB)
         for name in ("orc_force_fp64", "orc_force_f32"):
             getattr(L, name).argtypes = [C.c_int, C.c_double] + [_dp] * 13
             getattr(L, name).restype = None
         L.orc_force_rows_fp64.argtypes = [C.c_int, C.c_double] + [_dp] * 7 + [C.c_int, _ip, _dp]
+        L.orc_force_rows_f32.argtypes = [C.c_int, C.c_double] + [_dp] * 7 + [C.c_int, _ip, _dp]
         L.orc_potential_rows.argtypes = [C.c_int, C.c_double] + [_dp] * 4 + [C.c_int, _ip, _dp]
         L.orc_invsqrt2d.argtypes = [C.c_double]
         L.orc_invsqrt2d.restype = C.c_double
@@ -85,6 +87,8 @@ def lib():
                                         + [_dp] * 8 + [_dp])
         L.orc_force_jvp.argtypes = [C.c_int, C.c_double] + [_dp] * 8
         L.orc_hermite_tlm.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int] + [_dp] * 6
+        L.orc_plummer.argtypes = [C.c_int, C.c_uint64] + [_dp] * 7
+        L.orc_plummer.restype = None
         _lib = L
     return _lib
 
@@ -118,6 +122,8 @@ def ref(f32: bool = False):
         L.ref_bench_create.restype = C.c_void_p
         L.ref_bench_step.argtypes = [C.c_void_p, _dp]
         L.ref_bench_destroy.argtypes = [C.c_void_p]
+        L.orc_plummer.argtypes = [C.c_int, C.c_uint64] + [_dp] * 7
+        L.orc_plummer.restype = None
         _ref[key] = L
     return _ref[key]
 
@@ -140,12 +146,14 @@ def force(state: dict, eps2: float, precision: str = "fp64") -> np.ndarray:
     return out
 
 
-def force_rows(state: dict, eps2: float, rows) -> np.ndarray:
+def force_rows(state: dict, eps2: float, rows, precision: str = "fp64") -> np.ndarray:
+    """Direct sums for the given i-rows; precision "f32" uses the reference's
+    _F32 pair arithmetic (the accuracy floor of the mixed kernels)."""
     x, y, z, m, vx, vy, vz = _state(state)
     rows = np.ascontiguousarray(rows, dtype=np.int32)
     out = np.zeros((6, rows.size))
-    lib().orc_force_rows_fp64(x.size, eps2, *map(_p, (x, y, z, m, vx, vy, vz)), rows.size,
-                              rows.ctypes.data_as(_ip), _p(out))
+    f = lib().orc_force_rows_f32 if precision == "f32" else lib().orc_force_rows_fp64
+    f(x.size, eps2, *map(_p, (x, y, z, m, vx, vy, vz)), rows.size, rows.ctypes.data_as(_ip), _p(out))
     return out
 
 
@@ -170,6 +178,16 @@ def kinetic(state: dict) -> float:
 def potential(state: dict, eps2: float, compat: bool = False) -> float:
     x, y, z, m = _state(state)[:4]
     return lib().orc_potential(x.size, eps2, int(compat), _p(x), _p(y), _p(z), _p(m))
+
+
+def plummer(n: int, seed: int, from_reference_build: bool = False) -> dict:
+    """The benchmark's Plummer bodies (oracle/plummer.cpp), value for value
+    the engine's nbody_plummer; from the library in oracle/_ref when
+    `from_reference_build`, so that a CPU leg loads no other library."""
+    arrs = [np.zeros(n) for _ in range(7)]
+    L = ref() if from_reference_build else lib()
+    L.orc_plummer(int(n), int(seed), *map(_p, arrs))
+    return dict(zip(("x", "y", "z", "m", "vx", "vy", "vz"), arrs))
 
 
 def initialize(n: int, eps2: float = 1e-7) -> dict:

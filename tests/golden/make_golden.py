@@ -6,7 +6,7 @@ by oracle/Makefile into oracle/_ref/ (FP64 build and the -D_F32 build) and
 driven through oracle/ref_harness.cpp.  Run in a container that has the
 reference tree:
 
-    make -C oracle all && OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    make -C oracle all REF=<reference tree> && OMP_NUM_THREADS=1 python tests/golden/make_golden.py
 
 One thread makes the reference's OpenMP reductions sum in index order, so
 the fixtures are reproducible bit for bit.

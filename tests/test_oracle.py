@@ -122,3 +122,35 @@ def test_restatement_vs_reference_build(n, monkeypatch):
     rs, rd, rdt = O.ref_hermite_fixed(s, 2.5e-5, 3)
     os_, od, odt = O.hermite_fixed(s, EPS2_REF, 2.5e-5, 3)
     assert all(same(rs[k], os_[k]) for k in rs) and same(rd, od) and rdt == odt
+
+
+@pytest.mark.parametrize("n,seed", [(1, 1), (1000, 2), (65536, 1)])
+def test_oracle_plummer_equals_engine_plummer(n, seed):
+    """The CPU legs of the benchmark build their Plummer bodies with the
+    oracle's own sampler (oracle/plummer.cpp) so that they load no product
+    library; it must give the engine's nbody_plummer bodies value for value
+    (the library's host-side generator needs no GPU)."""
+    import nbody_b200 as nb
+    want = nb.plummer(n, seed)
+    got = O.plummer(n, seed)
+    for k in ("x", "y", "z", "m", "vx", "vy", "vz"):
+        assert same(got[k], want[k]), k
+    if O.have_reference():
+        got = O.plummer(n, seed, from_reference_build=True)
+        for k in ("x", "y", "z", "m", "vx", "vy", "vz"):
+            assert same(got[k], want[k]), k
+
+
+@pytest.mark.parametrize("n", (33, 1024))
+def test_f32_rows_equal_symmetric_f32_loop(n):
+    """The row-wise _F32 sum (large-N accuracy floor) gives the symmetric
+    _F32 loop's result up to the order of its double accumulation."""
+    g = golden(n)
+    s = state_of(g)
+    rows = np.arange(n)
+    d = O.force_rows(s, EPS2_REF, rows, "f32")
+    ref = g["force_f32"]
+    for blk in (slice(0, 3), slice(3, 6)):
+        num = np.sqrt(((d[blk] - ref[blk]) ** 2).sum(0))
+        den = np.sqrt((ref[blk] ** 2).sum(0))
+        assert (num / den).max() < 1e-13
