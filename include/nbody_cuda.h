@@ -70,12 +70,19 @@ typedef struct {
                          costs more than it saves), 1 = scalar FP32 kernel
                          on hi/lo positions, 2 = packed-pair (f32x2) hi/lo
                          kernel, FP64 accumulators in registers, 3 = packed
-                         hi/lo kernel, FP64 accumulators in shared memory
-                         (the most accurate), 4 = packed-pair kernel on
-                         tile-relative positions (Morton-ordered j-tiles,
-                         one add per separation component; the fastest
-                         for large systems)                                 */
-  int sort_every;     /* tile-relative kernel: re-order the j-bodies along
+                         hi/lo kernel, FP64 accumulators in shared memory,
+                         4 = near/far tile-relative packed-pair kernel: the
+                         engine keeps its bodies in Morton order and cuts
+                         them into j-tiles with float offsets from each
+                         tile's centre; a tile far from a warp's rows
+                         (separated by at least half its radius) costs one
+                         add per separation component, a near tile forms
+                         the separation in double-single (hi/lo offsets),
+                         so close pairs keep the hi/lo kernels' accuracy
+                         (the fastest for large systems), 5 = the same
+                         kernel with every tile taken as far (plain
+                         tile-relative offsets; a comparison)               */
+  int sort_every;     /* tile-relative kernels: re-order the bodies along
                          the Morton curve every this many steps (tile
                          centres and offsets are rebuilt every step);
                          0 = 16                                             */
@@ -94,10 +101,34 @@ typedef struct {
   double t, dt;                     /* model time and current shared dt     */
   int record_format;                /* j-records of the pair kernel in use:
                                        0 FP64, 1 FP32 hi/lo, 2 packed hi/lo,
-                                       3 packed tile-relative (Morton tiles) */
+                                       3 packed near/far tile-relative
+                                       (bodies kept in Morton order)       */
   int step_kernels;                 /* kernel launches in one captured step */
   long long reorders;               /* Morton re-orderings run by steps     */
   int order_kernels;                /* kernel launches in one re-ordering   */
+  double dt_crit;                   /* criterion of the last completed pass:
+                                       after a step, the Aarseth shared step
+                                       min_i sqrt(eta (|a||a2| + |j|^2) /
+                                       (|j||a3| + |a2|^2)) from the pre-step
+                                       a, j (src/nbody.cpp:198-222), computed
+                                       in fixed-dt mode too (where it is only
+                                       reported); after an adaptive-mode
+                                       nbody_acc_jerk, the initial criterion
+                                       min_i eta0 |a|/|j| (src/nbody.cpp:
+                                       131-150); 0 before either            */
+  int tiling_source;                /* how the tiling in use was chosen:
+                                       0 = not yet chosen, 1 = heuristic
+                                       (wave model) or explicit config,
+                                       2 = timed by the autotuner for this
+                                       engine, 3 = the autotuner's earlier
+                                       result for the same (device,
+                                       precision, kernel family, size),
+                                       reused from the process-wide cache  */
+  double near_tile_fraction;        /* near/far tile-relative kernel: share
+                                       of (warp, j-tile) pairs of the last
+                                       pair pass over this engine's bodies
+                                       that took the double-single (near)
+                                       form; 0 for other kernels            */
 } nbody_timers;
 
 /* Fill *cfg with defaults: eps2 = 1e-7, FP64, device 0, adaptive dt,
@@ -160,8 +191,10 @@ const char* nbody_status_string(nbody_status s);
  * 240-246) gets the complete result.  A cached engine per (thread, device)
  * is reused, so repeated calls allocate nothing after the first.  Copies
  * host->device and back inside the call (the reference contract).
- * precision = NBODY_MIXED: the tile-relative kernel from 32768 bodies (each
- * call re-orders the bodies), the packed hi/lo kernel below. */
+ * precision = NBODY_MIXED: the near/far tile-relative kernel from 32768
+ * bodies over the full row range (each call orders the bodies along the
+ * Morton curve in device memory and returns results in the caller's order),
+ * the packed hi/lo kernel below that and for partial row ranges. */
 nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin, int i_end,
                                      const double* x, const double* y, const double* z,
                                      const double* m, const double* vx, const double* vy,
@@ -189,14 +222,20 @@ nbody_status nbody_acc_jerk_device(nbody_engine* eng, int n, const double* x, co
  * its own pool, a real-time loop where cudaMalloc/cudaFree would stall the
  * device, code running inside someone else's time-step loop): same inputs,
  * outputs and physics as nbody_acc_jerk_device (mixed precision: the packed
- * hi/lo kernel, pair_variant 3), but no engine and no cudaMalloc - its scratch is a 16 MiB static device array inside the
- * library, held by every GPU that loads the library until the process exits.
- * n must be <= 32768 (NBODY_ERR_INVALID_ARG beyond).  Arrays are float64 on
- * the current device; work is enqueued on `stream` (cudaStream_t, NULL = the
- * legacy default stream) and the call returns without waiting.  The first
- * call on a device looks up the scratch address (cudaGetSymbolAddress); make
- * it before any stream capture.  All calls share the scratch: calls that
- * overlap on the GPU race; order them on one stream. */
+ * hi/lo kernel with FP64 accumulators in registers, pair_variant 2), but no
+ * engine and no cudaMalloc - its scratch is a 16 MiB static device array
+ * inside the library, held by every GPU that loads the library until the
+ * process exits.  n must be <= 32768 (NBODY_ERR_INVALID_ARG beyond).  Arrays
+ * are float64 on the current device; work is enqueued on `stream`
+ * (cudaStream_t, NULL = the legacy default stream) and the call returns
+ * without waiting.  Each call on a stream that is not capturing looks up the
+ * scratch address (cudaGetSymbolAddress); one on a capturing stream reuses
+ * the last lookup, so make the first call on a device before any stream
+ * capture.  All calls share the scratch: calls that overlap on the GPU race;
+ * order them on one stream.  Because the call does not wait, a bounded-wait
+ * timeout of its pair kernel cannot come back as a status: it shows up as NaN
+ * in all six outputs.  A CUDA error already pending in the calling thread is
+ * reported (NBODY_ERR_CUDA) and left in place; nothing is launched then. */
 nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision, const double* x,
                                     const double* y, const double* z, const double* m,
                                     const double* vx, const double* vy, const double* vz,
@@ -222,9 +261,11 @@ typedef struct {
   int tiles_per_item;    /* j-tiles per work item; 0 = default 8, or (with the
                             kernel shape) chosen by timing when tune = 1    */
   int tune;
-  int pair_variant;      /* mixed only: 0 = tile-relative packed kernel
-                            (per-cluster Morton tiles; default), 3 = packed
-                            hi/lo kernel (nbody_config numbering)          */
+  int pair_variant;      /* mixed only: 0 = near/far tile-relative kernel
+                            (each cluster kept in Morton order within its
+                            segment; default), 3 = packed hi/lo kernel,
+                            5 = tile-relative with every tile taken as far
+                            (nbody_config numbering)                       */
   int sort_every;        /* variant 0: re-order every this many steps; 0 = 16 */
 } nbody_ensemble_config;
 typedef struct {

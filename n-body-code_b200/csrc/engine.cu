@@ -6,17 +6,20 @@
 //   P      [S][6][ld]        split-j partial sums of the pair kernel
 //   jb64   [ld] JBody64      FP64 j-records (also used by the potential)
 //   jb32   [ld] JBody32      mixed-precision j-records (mixed engines):
-//                            JBody32, JBodyX2, or tiles of JBodyRel
-//   sort   keys, indices, order, CUB scratch of the Morton ordering that
-//          builds the JBodyRel tiles (mixed engines)
+//                            JBody32, JBodyX2, or tiles of JBodyNF
+//   sort   keys, indices, CUB scratch of the Morton ordering (mixed engines)
+//   perm   [2][ld] int       position -> caller's body index (tile-relative
+//                            engines keep their state in Morton order)
+//   scratch [13][ld]         re-ordered state, gathered caller input, or
+//                            output on its way back to the caller's order
 //   ctl    StepCtl           dt, t, Aarseth criterion, step counter
 // ld = n rounded up to a multiple of 256 (kPad).
 //
-// A Hermite step - predict (O(N), writes the j-records; the tile-relative
-// mixed kernel's records come from rel_tile_kernel right after), pair
-// (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
+// A Hermite step - predict (O(N), writes the j-records; the near/far
+// tile-relative kernel's records come from rel_tile_nf_kernel right after),
+// pair (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
 // correction + dt criterion) - is captured once into a CUDA graph and
-// replayed.  The Morton re-ordering of the tile-relative records is a
+// replayed.  The Morton re-ordering of a tile-relative engine's state is a
 // second captured graph, replayed ahead of every sort_every-th step.
 #include <cuda_runtime.h>
 
@@ -89,6 +92,7 @@ struct PairKernel {
   const void* fn;
   size_t smem;  // dynamic shared memory: two j-tile buffers (+ FP64 accumulators)
   int acc_smem = 0, junroll = 2, minb = 1;
+  int near = 0;  // tile-relative: 1 = near tiles in double-single (variant 4), 0 = all far (5)
 };
 
 template <int NT, int IPT, int TJ, int JU = 2, int MINB = 1>
@@ -109,12 +113,12 @@ PairKernel make_mixed_x2() {
           2 * TJ * sizeof(JBodyX2) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU, MINB};
 }
 
-template <int NT, int IPT, int TJ, int ACC = 1, int JU = 1, int MINB = 1>
-PairKernel make_mixed_rel() {
+template <int NT, int IPT, int TJ, int ACC = 1, int JU = 1, int MINB = 1, int NEAR = 1>
+PairKernel make_mixed_nf() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecRel,
-          reinterpret_cast<const void*>(&pair_mixed_rel_kernel<NT, IPT, TJ, ACC, JU, MINB>),
-          2 * (TJ + 1) * sizeof(JBodyRel) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU,
-          MINB};
+          reinterpret_cast<const void*>(&pair_mixed_nf_kernel<NT, IPT, TJ, ACC, JU, MINB, NEAR>),
+          2 * (TJ + 1) * sizeof(JBodyNF) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU,
+          MINB, NEAR};
 }
 
 // The first entry of each shape/variant is the one explicit tilings select;
@@ -125,14 +129,18 @@ const std::vector<PairKernel>& registry() {
       make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
       make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
       make_fp64<128, 2, 128, 1, 6>(), make_fp64<128, 2, 64, 1, 6>(), make_fp64<128, 1, 128, 4, 8>(),
-      // tile-relative packed pairs (Morton-ordered j-tiles; default mixed:
-      // 128 x 4 rows, j-unroll 2, 4 CTAs/SM = 128 registers, no spills)
-      make_mixed_rel<128, 4, 128, 1, 2, 4>(), make_mixed_rel<64, 4, 128>(), make_mixed_rel<128, 2, 128>(),
-      make_mixed_rel<256, 2, 128>(), make_mixed_rel<256, 4, 128>(), make_mixed_rel<128, 2, 64>(),
-      make_mixed_rel<128, 4, 64>(),  make_mixed_rel<128, 2, 256>(), make_mixed_rel<128, 4, 128, 0, 2>(),
-      make_mixed_rel<128, 4, 128>(), make_mixed_rel<128, 4, 128, 1, 1, 4>(),
-      make_mixed_rel<64, 4, 128, 1, 1, 8>(),  make_mixed_rel<128, 6, 128, 1, 1>(),
-      make_mixed_rel<64, 6, 128, 1, 1>(),     make_mixed_rel<128, 4, 128, 1, 2>(),
+      // near/far tile-relative packed pairs (bodies in Morton order; default
+      // mixed: 128 x 4 rows, j-unroll 2, 4 CTAs/SM = 128 registers, no spills)
+      make_mixed_nf<128, 4, 128, 1, 2, 4>(), make_mixed_nf<64, 4, 128>(), make_mixed_nf<128, 2, 128>(),
+      make_mixed_nf<256, 2, 128>(), make_mixed_nf<256, 4, 128>(), make_mixed_nf<128, 2, 64>(),
+      make_mixed_nf<128, 4, 64>(),  make_mixed_nf<128, 2, 256>(), make_mixed_nf<128, 4, 128, 0, 2>(),
+      make_mixed_nf<128, 4, 128>(), make_mixed_nf<128, 4, 128, 1, 1, 4>(),
+      make_mixed_nf<64, 4, 128, 1, 1, 8>(),  make_mixed_nf<128, 6, 128, 1, 1>(),
+      make_mixed_nf<64, 6, 128, 1, 1>(),     make_mixed_nf<128, 4, 128, 1, 2>(),
+      make_mixed_nf<128, 4, 64, 1, 2, 4>(),  make_mixed_nf<128, 2, 64, 1, 2, 4>(),
+      // the same kernel with every tile taken as far (plain tile-relative
+      // separations; pair_variant 5, a measured comparison)
+      make_mixed_nf<128, 4, 128, 1, 2, 4, 0>(), make_mixed_nf<128, 2, 128, 1, 1, 1, 0>(),
       // packed pairs, FP64 accumulators in shared memory (default)
       make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
       make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
@@ -153,18 +161,21 @@ const std::vector<PairKernel>& registry() {
 // variant (mixed only, after resolving 0 = automatic): 1 = scalar FP32
 // hi/lo, 2 = packed hi/lo pairs with register accumulators, 3 = packed
 // hi/lo pairs with shared-memory FP64 accumulators (falling back to
-// register accumulators where that shape has none), 4 = tile-relative.
+// register accumulators where that shape has none), 4 = near/far
+// tile-relative, 5 = tile-relative with every tile taken as far.
 const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
-  auto match = [&](int fmt, int acc) -> const PairKernel* {
+  auto match = [&](int fmt, int acc, int near = 1) -> const PairKernel* {
     for (const auto& k : registry())
       if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj &&
-          (fmt < 0 || k.fmt == fmt) && (acc < 0 || k.acc_smem == acc))
+          (fmt < 0 || k.fmt == fmt) && (acc < 0 || k.acc_smem == acc) &&
+          (k.fmt != kRecRel || k.near == near))
         return &k;
     return nullptr;
   };
   if (precision == NBODY_FP64) return match(kRecF64, -1);
   if (variant == 1) return match(kRecF32, -1);
-  if (variant == 4) return match(kRecRel, -1);
+  if (variant == 4) return match(kRecRel, -1, 1);
+  if (variant == 5) return match(kRecRel, -1, 0);
   if (variant == 2) return match(kRecX2, 0);
   const PairKernel* k = match(kRecX2, 1);
   return k ? k : match(kRecX2, 0);
@@ -174,12 +185,13 @@ const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int varian
 struct Tiling {
   const PairKernel* k = nullptr;
   int split = 1;
+  int source = 0;  // nbody_timers.tiling_source: 1 heuristic/explicit, 2 timed, 3 cached
 };
 
 // Autotune results shared by all engines of the process: (device, precision,
-// ld, rows) -> tiling.
+// record format, ld, rows) -> tiling.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;  // -> (kernel idx, split)
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_tuned;  // -> (kernel idx, split)
 
 }  // namespace
 
@@ -204,14 +216,19 @@ struct nbody_engine {
   JBody64* jb64 = nullptr;
   void* jb32 = nullptr;  // mixed records: JBody32 or JBodyX2 (sized for the larger)
   JBody64* jbe = nullptr;  // records of the energy diagnostic (never a pair kernel's input)
-  // Morton ordering of the tile-relative records (mixed engines)
+  // Morton ordering (mixed engines).  A tile-relative engine keeps its state
+  // in Morton order: position p holds the caller's body perm[p].
   uint64_t* sort_keys = nullptr;  // [2][ld]: keys, sorted keys
-  int* sort_idx = nullptr;        // [2][ld]: indices, sorted indices (= order)
+  int* sort_idx = nullptr;        // [2][ld]: positions, sorted positions (= order)
   double* bbox_part = nullptr;    // [kMaxBBoxParts][6]
   void* sort_tmp = nullptr;
   size_t sort_tmp_bytes = 0;
-  bool order_own = false;         // the order is of this engine's own n bodies
-  int since_sort = 0;             // steps since that order was made
+  int* perm = nullptr;            // [2][ld]: position -> body index, and its re-ordered copy
+  double* scratch = nullptr;      // [13][ld]: re-ordered state / gathered caller input / un-permuted output
+  unsigned long long* near_count = nullptr;  // near tiles of the last near/far pair launch
+  bool sorted = false;            // the state is in (recent) Morton order
+  bool permuted = false;          // perm is not the identity
+  int since_sort = 0;             // steps since the last re-ordering
   StepCtl* ctl = nullptr;
   double* partial = nullptr;  // reduction scratch: ld / 256 + 1 doubles + 4 scalars
   int* status = nullptr;
@@ -249,8 +266,11 @@ int effective_variant(const nbody_engine* e) {
 // Record format of the autotuner's family (the automatic choice).
 int default_format(const nbody_engine* e) {
   if (e->cfg.precision == NBODY_FP64) return kRecF64;
-  return effective_variant(e) == 4 ? kRecRel : kRecX2;
+  return effective_variant(e) >= 4 ? kRecRel : kRecX2;
 }
+
+// The engine keeps its bodies in Morton order (positions != body indices).
+bool morton_resident(const nbody_engine* e);
 
 nbody_status check_status_word(nbody_engine* e) {
   int h = 0;
@@ -344,6 +364,10 @@ nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_en
     const SoA7 in = src ? *src : own_inputs(e);
     a.rows = RowSrc{in.x, in.y, in.z, in.vx, in.vy, in.vz};
     a.n_rows_pad = src ? n_src : e->n;
+    if (k.near && i_end > i_begin) {  // count this launch's near tiles
+      NB_CUDA(cudaMemsetAsync(e->near_count, 0, sizeof(unsigned long long), st));
+      a.near_count = e->near_count;
+    }
   }
   a.n_tiles = e->ld / k.tj;
   a.tiles_per_split = (a.n_tiles + t.split - 1) / t.split;
@@ -363,15 +387,17 @@ nbody_status launch_pair(nbody_engine* e, const Tiling& t, int i_begin, int i_en
 
 nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
                          int tj);
+nbody_status enqueue_reorder_state(nbody_engine* e, cudaStream_t st);
 
 nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
-  const auto key = std::make_tuple(e->dev, e->cfg.precision, e->ld, rows);
+  const auto key = std::make_tuple(e->dev, e->cfg.precision, default_format(e), e->ld, rows);
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) {
       out->k = &registry()[it->second.first];
       out->split = it->second.second;
+      out->source = 3;
       return NBODY_OK;
     }
   }
@@ -381,9 +407,13 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   float best = 1e30f;
   int best_idx = -1, best_split = 1;
   const auto& reg = registry();
+  // the near/far kernel's cost depends on the bodies being in Morton order
+  if (default_format(e) == kRecRel && e->have_state && !e->sorted)
+    NB_TRY(enqueue_reorder_state(e, e->stream));
   for (size_t idx = 0; idx < reg.size(); ++idx) {
     const PairKernel& k = reg[idx];
     if (k.precision != e->cfg.precision || k.fmt != default_format(e)) continue;
+    if (k.fmt == kRecRel && !k.near) continue;  // the automatic choice keeps near tiles exact
     const int s0 = choose_split(e, k, rows);
     NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt, k.tj));
     for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
@@ -412,6 +442,7 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   if (best_idx < 0) return fail(NBODY_ERR_STATE, "autotune found no kernel");
   out->k = &reg[best_idx];
   out->split = best_split;
+  out->source = 2;
   std::lock_guard<std::mutex> g(g_tune_mu);
   g_tuned[key] = {best_idx, best_split};
   return NBODY_OK;
@@ -440,6 +471,17 @@ nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
     return autotune(e, rows, out);
   out->k = k;
   out->split = c.split_j ? std::min(c.split_j, kMaxSplit) : choose_split(e, *k, rows);
+  out->source = 1;
+  return NBODY_OK;
+}
+
+// The packed hi/lo kernel (pair_variant 3) for `rows` rows, heuristic split.
+nbody_status hilo_tiling(nbody_engine* e, int rows, Tiling* out) {
+  const PairKernel* k = find_kernel(NBODY_MIXED, 128, 2, 128, 3);
+  if (!k) return fail(NBODY_ERR_STATE, "no packed hi/lo kernel compiled");
+  out->k = k;
+  out->split = choose_split(e, *k, rows);
+  out->source = 1;
   return NBODY_OK;
 }
 
@@ -460,10 +502,10 @@ SoA6 own_derivs(nbody_engine* e) {
   return SoA6{D, D + ld, D + 2 * ld, D + 3 * ld, D + 4 * ld, D + 5 * ld};
 }
 
-// Morton order of bodies [0, n) of `in` (bounding box, keys, stable sort)
-// into sort_idx + ld; own = the inputs are the engine's state.
-nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st,
-                                  bool own) {
+// Morton order of bodies [0, n) of `in` (bounding box, keys, stable sort):
+// sort_idx + ld then holds, for each sorted position q, the index in `in` of
+// the body that goes there.
+nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
   const int parts = std::min(kMaxBBoxParts, (n + kBBoxThreads - 1) / kBBoxThreads);
   bbox_partial_kernel<<<parts, kBBoxThreads, 0, st>>>(n, in, e->bbox_part);
   NB_CUDA(cudaGetLastError());
@@ -474,21 +516,46 @@ nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaSt
   size_t bytes = e->sort_tmp_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + ld,
                                           e->sort_idx, e->sort_idx + ld, n, 0, kMortonBits, st));
-  e->order_own = own && n == e->n;
+  return NBODY_OK;
+}
+
+GatherArgs gather_args(const double* src, double* dst, size_t ld, int arrays) {
+  GatherArgs g;
+  g.arrays = arrays;
+  for (int a = 0; a < kMaxGather; ++a) {
+    g.src[a] = a < arrays && src ? src + a * ld : nullptr;
+    g.dst[a] = a < arrays ? dst + a * ld : nullptr;
+  }
+  return g;
+}
+
+// Re-orders the engine's own state into the Morton order of its current
+// positions: keys and sort, a gather of all 13 state arrays (and of perm)
+// into scratch, and a copy back.  Capturable (the re-ordering graph).
+nbody_status enqueue_reorder_state(nbody_engine* e, cudaStream_t st) {
+  const size_t ld = e->ld;
+  NB_TRY(enqueue_morton_order(e, e->n, own_inputs(e), st));
+  gather_rows_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      e->n, e->sort_idx + ld, gather_args(e->state, e->scratch, ld, 13), e->perm, e->perm + ld);
+  NB_CUDA(cudaGetLastError());
+  // scratch rows >= n are zero from creation and never written, so the padding stays zero
+  NB_CUDA(cudaMemcpyAsync(e->state, e->scratch, sizeof(double) * 13 * ld, cudaMemcpyDeviceToDevice, st));
+  NB_CUDA(cudaMemcpyAsync(e->perm, e->perm + ld, sizeof(int) * e->n, cudaMemcpyDeviceToDevice, st));
+  e->sorted = true;
+  e->permuted = true;
   e->since_sort = 0;
   return NBODY_OK;
 }
 
-// Tiles of tj tile-relative records of bodies [0, n) of `in`, in the order
-// of the last enqueue_morton_order.
+// Near/far tile records of bodies [0, n) of `in`, which must already be in
+// Morton order (positions).
 nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int tj) {
-  const int* order = e->sort_idx + e->ld;
-  JBodyRel* out = static_cast<JBodyRel*>(e->jb32);
+  JBodyNF* out = static_cast<JBodyNF*>(e->jb32);
   const int tiles = e->ld / tj;
   switch (tj) {
-    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(n, in, order, out, nullptr); break;
-    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(n, in, order, out, nullptr); break;
-    case 256: rel_tile_kernel<256><<<tiles, 256, 0, st>>>(n, in, order, out, nullptr); break;
+    case 64: rel_tile_nf_kernel<64><<<tiles, 64, 0, st>>>(n, in, out); break;
+    case 128: rel_tile_nf_kernel<128><<<tiles, 128, 0, st>>>(n, in, out); break;
+    case 256: rel_tile_nf_kernel<256><<<tiles, 256, 0, st>>>(n, in, out); break;
     default: return fail(NBODY_ERR_INVALID_ARG, "no tile-relative record builder for j_tile %d", tj);
   }
   NB_CUDA(cudaGetLastError());
@@ -496,8 +563,8 @@ nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_
 }
 
 // Writes the j-records of a pair kernel's format: FP64 records (hi/lo
-// kernels: also theirs), or tiles of tj tile-relative records, re-ordered
-// first.  (The energy diagnostic packs its own records.)
+// kernels: also theirs), or tiles of tj near/far records of `in`, which must
+// then be in Morton order.  (The energy diagnostic packs its own records.)
 nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
                          int tj) {
   if (fmt != kRecRel) {
@@ -506,9 +573,31 @@ nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st
         fmt == kRecX2 ? static_cast<JBodyX2*>(e->jb32) : nullptr);
     NB_CUDA(cudaGetLastError());
   } else {
-    NB_TRY(enqueue_morton_order(e, n, in, st, in.x == e->X));
     NB_TRY(build_rel_tiles(e, n, in, st, tj));
   }
+  return NBODY_OK;
+}
+
+// acc + jerk of n bodies given in any order (`in`, device arrays) with the
+// near/far kernel, after enqueue_morton_order(in): a gather of `in` into
+// scratch in that order, tiles, the pair pass, and the split reduction
+// written back through the order into `out` (the caller's body order).
+// Leaves the engine's own state alone.
+nbody_status eval_foreign_rel(nbody_engine* e, const Tiling& t, int n, const SoA7& in,
+                              const SoA6& out, cudaStream_t st) {
+  const size_t ld = e->ld;
+  const int* ord = e->sort_idx + ld;
+  const double* srcs[7] = {in.x, in.y, in.z, in.m, in.vx, in.vy, in.vz};
+  GatherArgs g = gather_args(nullptr, e->scratch, ld, 7);
+  for (int a = 0; a < 7; ++a) g.src[a] = srcs[a];
+  gather_rows_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(n, ord, g, nullptr, nullptr);
+  NB_CUDA(cudaGetLastError());
+  const SoA7 sorted{g.dst[0], g.dst[1], g.dst[2], g.dst[3], g.dst[4], g.dst[5], g.dst[6]};
+  NB_TRY(build_rel_tiles(e, n, sorted, st, t.k->tj));
+  NB_TRY(launch_pair(e, t, 0, n, st, &sorted, n));
+  reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
+      0, n, e->ld, t.split, e->P, out, nullptr, ord);
+  NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
 
@@ -516,17 +605,20 @@ int tiling_fmt(const nbody_engine* e) { return e->tiled ? e->tiling.k->fmt : kRe
 int tiling_tj(const nbody_engine* e) { return e->tiled ? e->tiling.k->tj : 0; }
 int sort_period(const nbody_engine* e) { return e->cfg.sort_every > 0 ? e->cfg.sort_every : 16; }
 
+bool morton_resident(const nbody_engine* e) { return tiling_fmt(e) == kRecRel; }
+
 // Before a step of the engine's own state: re-order when the order is stale
-// (another system's, or sort_every steps old).
+// (never made since set_state, or sort_every steps old).
 nbody_status maybe_reorder(nbody_engine* e, cudaStream_t st) {
-  if (tiling_fmt(e) != kRecRel) return NBODY_OK;
-  if (!e->order_own || e->since_sort >= sort_period(e)) {
+  if (!morton_resident(e)) return NBODY_OK;
+  if (!e->sorted || e->since_sort >= sort_period(e)) {
     if (e->order_graph && st == e->stream) {
       NB_CUDA(cudaGraphLaunch(e->order_graph, st));
-      e->order_own = true;
+      e->sorted = true;
+      e->permuted = true;
       e->since_sort = 0;
     } else {
-      NB_TRY(enqueue_morton_order(e, e->n, own_inputs(e), st, true));
+      NB_TRY(enqueue_reorder_state(e, st));
     }
     ++e->reorders;
   }
@@ -537,6 +629,7 @@ nbody_status maybe_reorder(nbody_engine* e, cudaStream_t st) {
 // acc + jerk of the engine's current X, V, M into D (rows [0, n)).
 nbody_status eval_current(nbody_engine* e) {
   NB_TRY(ensure_tiling(e));
+  if (morton_resident(e) && !e->sorted) NB_TRY(enqueue_reorder_state(e, e->stream));
   NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   if (!e->init_events) {
     NB_CUDA(cudaEventCreate(&e->ev_init[0]));
@@ -628,13 +721,14 @@ nbody_status build_step_graph(nbody_engine* e) {
   if (tiling_fmt(e) == kRecRel && !e->order_graph) {
     // the Morton re-ordering of the engine's own state, replayed every
     // sort_every steps ahead of the step graph
-    const bool own = e->order_own;
+    const bool sorted = e->sorted, permuted = e->permuted;
     const int since = e->since_sort;
     NB_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-    s = enqueue_morton_order(e, e->n, own_inputs(e), e->stream, true);
+    s = enqueue_reorder_state(e, e->stream);
     g = nullptr;
     ce = cudaStreamEndCapture(e->stream, &g);
-    e->order_own = own;  // capturing ran nothing
+    e->sorted = sorted;  // capturing ran nothing
+    e->permuted = permuted;
     e->since_sort = since;
     if (s != NBODY_OK) {
       if (g) cudaGraphDestroy(g);
@@ -715,7 +809,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
   if (!(cfg->eta > 0) || !(cfg->eta0 > 0)) return fail(NBODY_ERR_INVALID_ARG, "eta/eta0 must be > 0");
   if (cfg->split_j < 0 || cfg->threads < 0 || cfg->i_per_thread < 0 || cfg->j_tile < 0)
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
-  if (cfg->pair_variant < 0 || cfg->pair_variant > 4)
+  if (cfg->pair_variant < 0 || cfg->pair_variant > 5)
     return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
   if (cfg->sort_every < 0) return fail(NBODY_ERR_INVALID_ARG, "sort_every = %d", cfg->sort_every);
   int ndev = 0;
@@ -752,8 +846,16 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
     NB_CUDA(cudaMalloc(&e->jb64, sizeof(JBody64) * ld));
     NB_CUDA(cudaMalloc(&e->jbe, sizeof(JBody64) * ld));
     if (cfg->precision == NBODY_MIXED) {
-      static_assert(sizeof(JBodyX2) >= sizeof(JBodyRel) * 65 / 64, "jb32 holds tiles of >= 64");
-      NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyX2) * ld));
+      // JBodyX2 records, or tiles of TJ + 1 JBodyNF records (TJ >= 64)
+      static_assert(sizeof(JBodyNF) >= sizeof(JBodyX2), "jb32 sized by the larger record");
+      NB_CUDA(cudaMalloc(&e->jb32, sizeof(JBodyNF) * (ld / 64) * 65));
+      NB_CUDA(cudaMalloc(&e->perm, sizeof(int) * 2 * ld));
+      iota_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(e->n, e->perm);
+      NB_CUDA(cudaGetLastError());
+      NB_CUDA(cudaMalloc(&e->scratch, sizeof(double) * 13 * ld));
+      NB_CUDA(cudaMemsetAsync(e->scratch, 0, sizeof(double) * 13 * ld, e->stream));
+      NB_CUDA(cudaMalloc(&e->near_count, sizeof(unsigned long long)));
+      NB_CUDA(cudaMemsetAsync(e->near_count, 0, sizeof(unsigned long long), e->stream));
       NB_CUDA(cudaMalloc(&e->sort_keys, sizeof(uint64_t) * 2 * ld));
       NB_CUDA(cudaMalloc(&e->sort_idx, sizeof(int) * 2 * ld));
       NB_CUDA(cudaMalloc(&e->bbox_part, sizeof(double) * 6 * kMaxBBoxParts));
@@ -794,6 +896,9 @@ nbody_status nbody_destroy(nbody_engine* e) {
   cudaFree(e->jbe);
   cudaFree(e->sort_keys);
   cudaFree(e->sort_idx);
+  cudaFree(e->perm);
+  cudaFree(e->scratch);
+  cudaFree(e->near_count);
   cudaFree(e->bbox_part);
   cudaFree(e->sort_tmp);
   cudaFree(e->ctl);
@@ -826,23 +931,44 @@ nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, 
   c.steps = 0;
   NB_CUDA(cudaMemcpyAsync(e->ctl, &c, sizeof c, cudaMemcpyHostToDevice, e->stream));
   NB_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * ld, e->stream));
-  NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
+  if (e->perm) {  // body order again; a tile-relative engine re-orders at its next evaluation
+    iota_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(e->n, e->perm);
+    NB_CUDA(cudaGetLastError());
+  }
+  e->sorted = e->permuted = false;
+  if (!morton_resident(e))
+    NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   NB_CUDA(cudaStreamSynchronize(e->stream));
   e->have_state = true;
   e->have_derivs = false;
   return NBODY_OK;
 }
 
+namespace {
+// Downloads `count` [ld] arrays starting at `src` (engine positions) to the
+// caller's arrays in body order: through scratch when the state is permuted.
+nbody_status download_rows(nbody_engine* e, const double* src, double* const* dst, int count) {
+  const size_t ld = e->ld, b = sizeof(double) * e->n;
+  const double* from = src;
+  if (e->permuted) {
+    scatter_rows_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+        e->n, e->perm, gather_args(src, e->scratch, ld, count));
+    NB_CUDA(cudaGetLastError());
+    from = e->scratch;
+  }
+  for (int k = 0; k < count; ++k)
+    if (dst[k]) NB_CUDA(cudaMemcpyAsync(dst[k], from + k * ld, b, cudaMemcpyDeviceToHost, e->stream));
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return NBODY_OK;
+}
+}  // namespace
+
 nbody_status nbody_get_state(nbody_engine* e, double* x, double* y, double* z, double* vx,
                              double* vy, double* vz) {
   TraceRange trace_("nbody_get_state");
   NB_TRY(need_state(e));
-  const size_t ld = e->ld, b = sizeof(double) * e->n;
   double* dst[6] = {x, y, z, vx, vy, vz};
-  const double* src[6] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld};
-  for (int k = 0; k < 6; ++k)
-    if (dst[k]) NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyDeviceToHost, e->stream));
-  NB_CUDA(cudaStreamSynchronize(e->stream));
+  NB_TRY(download_rows(e, e->X, dst, 6));  // X(3) and V(3) are consecutive state arrays
   return check_status_word(e);
 }
 
@@ -850,11 +976,8 @@ nbody_status nbody_get_derivs(nbody_engine* e, double* ax, double* ay, double* a
                               double* jy, double* jz) {
   NB_TRY(need_state(e));
   if (!e->have_derivs) return fail(NBODY_ERR_STATE, "no derivatives yet (call nbody_acc_jerk)");
-  const size_t ld = e->ld, b = sizeof(double) * e->n;
   double* dst[6] = {ax, ay, az, jx, jy, jz};
-  for (int k = 0; k < 6; ++k)
-    if (dst[k]) NB_CUDA(cudaMemcpyAsync(dst[k], e->D + k * ld, b, cudaMemcpyDeviceToHost, e->stream));
-  NB_CUDA(cudaStreamSynchronize(e->stream));
+  NB_TRY(download_rows(e, e->D, dst, 6));
   return check_status_word(e);
 }
 
@@ -951,6 +1074,16 @@ nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
     out->j_tile = e->tiling.k->tj;
     out->split_j = e->tiling.split;
     out->record_format = e->tiling.k->fmt;
+    out->tiling_source = e->tiling.source;
+    const PairKernel& k = *e->tiling.k;
+    if (k.fmt == kRecRel && k.near) {
+      unsigned long long near = 0;
+      NB_CUDA(cudaMemcpy(&near, e->near_count, sizeof near, cudaMemcpyDeviceToHost));
+      // classified per (warp, tile): warps = row blocks x NT / 32
+      const double pairs = static_cast<double>((e->n + k.nt * k.ipt - 1) / (k.nt * k.ipt)) *
+                           (k.nt / 32) * static_cast<double>(e->ld / k.tj);
+      out->near_tile_fraction = static_cast<double>(near) / pairs;
+    }
   }
   out->step_kernels = e->graph_kernels;
   out->reorders = e->reorders;
@@ -961,6 +1094,7 @@ nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
     out->steps = c.steps;
     out->t = c.t;
     out->dt = c.dt;
+    out->dt_crit = c.dt_crit;
   }
   return NBODY_OK;
 }
@@ -999,10 +1133,15 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   NB_TRY(get_tiling(e, n, &t));
   NB_TRY(ensure_partials(e, t.split));
   const SoA7 in{x, y, z, m, vx, vy, vz};
+  const SoA6 out{ax, ay, az, jx, jy, jz};
+  if (t.k->fmt == kRecRel) {  // Morton order of the caller's bodies, gathered into scratch
+    NB_TRY(enqueue_morton_order(e, n, in, st));
+    return eval_foreign_rel(e, t, n, in, out, st);
+  }
   NB_TRY(launch_pack(e, n, in, st, t.k->fmt, t.k->tj));
   NB_TRY(launch_pair(e, t, 0, n, st, &in, n));
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      0, n, e->ld, t.split, e->P, SoA6{ax, ay, az, jx, jy, jz});
+      0, n, e->ld, t.split, e->P, out);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
@@ -1069,7 +1208,11 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};
   NB_TRY(ensure_tiling(e));
   Tiling t = e->tiling;
-  if (i_end - i_begin != n) NB_TRY(get_tiling(e, i_end - i_begin, &t));
+  const bool full = i_begin == 0 && i_end == n;
+  if (!full) NB_TRY(get_tiling(e, i_end - i_begin, &t));
+  // a row range: the packed hi/lo kernel, whose rows stay in the caller's
+  // order (the near/far kernel evaluates all rows in Morton order)
+  if (!full && t.k->fmt == kRecRel) NB_TRY(hilo_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
   if (t.k->fmt == kRecRel) {
     // positions first: their Morton ordering runs while the masses and
@@ -1085,19 +1228,20 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     for (int k = 3; k < 7; ++k)
       NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->aux));
     NB_CUDA(cudaEventRecord(e->aux_ev[1], e->aux));
-    NB_TRY(enqueue_morton_order(e, n, own_inputs(e), e->stream, true));
+    NB_TRY(enqueue_morton_order(e, n, own_inputs(e), e->stream));
     NB_CUDA(cudaStreamWaitEvent(e->stream, e->aux_ev[1], 0));
-    NB_TRY(build_rel_tiles(e, n, own_inputs(e), e->stream, t.k->tj));
+    // the caller's bodies gathered into Morton order, derivatives back in body order
+    NB_TRY(eval_foreign_rel(e, t, n, own_inputs(e), own_derivs(e), e->stream));
   } else {
     for (int k = 0; k < 7; ++k)
       NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
     NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt, t.k->tj));
-  }
-  NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
-  if (i_end > i_begin) {
-    reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
-        i_begin, i_end, e->ld, t.split, e->P, own_derivs(e));
-    NB_CUDA(cudaGetLastError());
+    NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
+    if (i_end > i_begin) {
+      reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+          i_begin, i_end, e->ld, t.split, e->P, own_derivs(e));
+      NB_CUDA(cudaGetLastError());
+    }
   }
   double* out[6] = {ax, ay, az, jx, jy, jz};
   const size_t rb = sizeof(double) * (i_end - i_begin);

@@ -261,6 +261,7 @@ struct EnsKernel {
   int fmt;  // RecordFormat of its j-records
   const void* fn;
   size_t smem;
+  int near = 0;  // tile-relative: 1 = near tiles in double-single, 0 = every tile far
 };
 
 template <class R>
@@ -271,25 +272,27 @@ EnsKernel ens_kernel(int precision) {
 }
 
 template <class R>
-EnsKernel ens_kernel_rel() {
+EnsKernel ens_kernel_nf() {
   static_assert(R::ROWS == kPadRows, "an item's row block is one padding unit");
   return {NBODY_MIXED, R::NT, R::TJ, kRecRel,
-          reinterpret_cast<const void*>(&ensemble_pair_rel_kernel<R>),
-          2 * (R::TJ + 1) * sizeof(JBodyRel) + R::kExtraSmem};
+          reinterpret_cast<const void*>(&ensemble_pair_nf_kernel<R>),
+          2 * (R::TJ + 1) * sizeof(JBodyNF) + R::kExtraSmem, R::kNear};
 }
 
-// The first entry of each (precision, record format) is its default.
+// The first entry of each (precision, record format, near) is its default.
 const std::vector<EnsKernel>& ens_registry() {
   static const std::vector<EnsKernel> r = {
       ens_kernel<RowsFP64<128, 2, 128, 1>>(NBODY_FP64),
       ens_kernel<RowsFP64<256, 1, 128, 4>>(NBODY_FP64),
-      ens_kernel_rel<RowsMixedRel<64, 4, 64, 1, 1>>(),
-      ens_kernel_rel<RowsMixedRel<64, 4, 128, 1, 1>>(),
-      ens_kernel_rel<RowsMixedRel<128, 2, 128, 1, 1>>(),
-      ens_kernel_rel<RowsMixedRel<128, 2, 64, 1, 1>>(),
-      ens_kernel_rel<RowsMixedRel<64, 4, 64, 1, 2>>(),
-      ens_kernel_rel<RowsMixedRel<128, 2, 128, 1, 2>>(),
-      ens_kernel_rel<RowsMixedRel<64, 4, 128, 1, 2>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 1>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 128, 1, 1, 1>>(),
+      ens_kernel_nf<RowsMixedNF<128, 2, 128, 1, 1, 1>>(),
+      ens_kernel_nf<RowsMixedNF<128, 2, 64, 1, 1, 1>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 2, 1>>(),
+      ens_kernel_nf<RowsMixedNF<128, 2, 128, 1, 2, 1>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 128, 1, 2, 1>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 0>>(),
+      ens_kernel_nf<RowsMixedNF<128, 2, 128, 1, 1, 0>>(),
       ens_kernel<RowsMixedX2<64, 4, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<128, 2, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<64, 4, 64, 1, 1>>(NBODY_MIXED),
@@ -329,7 +332,13 @@ struct nbody_ensemble {
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool have_derivs = false;
   long long steps = 0;
-  // Morton ordering of the tile-relative records (mixed, variant 0)
+  // Morton ordering (mixed, tile-relative variants): each cluster keeps its
+  // bodies in Morton order within its segment; position r holds the body of
+  // padded row perm[r] (the caller's order).
+  int near = 1;                   // near/far kernel (variant 0) or every tile far (5)
+  int* perm = nullptr;            // [2][L]
+  double* scratch = nullptr;      // [13][L]
+  bool sorted = false, permuted = false;
   int* seg = nullptr;             // [L] cluster owning each padded row
   double* bbox = nullptr;         // [C][6]
   uint64_t* sort_keys = nullptr;  // [2][L]
@@ -429,19 +438,69 @@ nbody_status ens_order(nbody_ensemble* e, cudaStream_t st) {
   return NBODY_OK;
 }
 
-// Tile-relative records (tiles of the kernel's TJ) in the last order.
+// Puts every cluster's bodies into Morton order within its segment: the
+// order of ens_order, a gather of all 13 state arrays (and of perm) into
+// scratch, and a copy back.  Capturable (the re-ordering graph).
+nbody_status ens_reorder_state(nbody_ensemble* e, cudaStream_t st) {
+  const size_t L = e->L;
+  EN_TRY(ens_order(e, st));
+  GatherArgs g;
+  g.arrays = 13;
+  for (int a = 0; a < 13; ++a) {
+    g.src[a] = e->state + a * L;
+    g.dst[a] = e->scratch + a * L;
+  }
+  gather_rows_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, st>>>(e->L, e->sort_idx + L, g,
+                                                                     e->perm, e->perm + L);
+  EN_CUDA(cudaGetLastError());
+  EN_CUDA(cudaMemcpyAsync(e->state, e->scratch, sizeof(double) * 13 * L, cudaMemcpyDeviceToDevice, st));
+  EN_CUDA(cudaMemcpyAsync(e->perm, e->perm + L, sizeof(int) * L, cudaMemcpyDeviceToDevice, st));
+  e->sorted = e->permuted = true;
+  e->since_sort = 0;
+  return NBODY_OK;
+}
+
+// Near/far tile records (tiles of the kernel's TJ) of the state, which is in
+// Morton order within each cluster segment.
 nbody_status ens_tiles(nbody_ensemble* e, cudaStream_t st) {
   const size_t L = e->L;
   const SoA7 in{e->X, e->X + L, e->X + 2 * L, e->M, e->V, e->V + L, e->V + 2 * L};
-  const int* order = e->sort_idx + L;
-  JBodyRel* out = reinterpret_cast<JBodyRel*>(e->jbx);
+  JBodyNF* out = reinterpret_cast<JBodyNF*>(e->jbx);
   const int tiles = e->L / e->kern->tile;
   switch (e->kern->tile) {
-    case 64: rel_tile_kernel<64><<<tiles, 64, 0, st>>>(e->L, in, order, out, e->cid); break;
-    case 128: rel_tile_kernel<128><<<tiles, 128, 0, st>>>(e->L, in, order, out, e->cid); break;
+    case 64: rel_tile_nf_kernel<64><<<tiles, 64, 0, st>>>(e->L, in, out, e->cid); break;
+    case 128: rel_tile_nf_kernel<128><<<tiles, 128, 0, st>>>(e->L, in, out, e->cid); break;
     default: return nbody_set_error(NBODY_ERR_INVALID_ARG, "no record builder for tile %d", e->kern->tile);
   }
   EN_CUDA(cudaGetLastError());
+  return NBODY_OK;
+}
+
+// Copies `count` [L] arrays starting at src to the caller's concatenated
+// arrays (cluster c's n_c bodies in turn), through scratch when permuted.
+nbody_status ens_download(nbody_ensemble* e, const double* src, double* const* dst, int count) {
+  const size_t L = e->L;
+  const double* from = src;
+  if (e->permuted) {
+    GatherArgs g;
+    g.arrays = count;
+    for (int a = 0; a < count; ++a) {
+      g.src[a] = src + a * L;
+      g.dst[a] = e->scratch + a * L;
+    }
+    scatter_rows_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->perm, g);
+    EN_CUDA(cudaGetLastError());
+    from = e->scratch;
+  }
+  long long off = 0;
+  for (int c = 0; c < e->C; ++c) {
+    for (int k = 0; k < count; ++k)
+      if (dst[k])
+        EN_CUDA(cudaMemcpyAsync(dst[k] + off, from + k * L + e->row0[c], sizeof(double) * e->n[c],
+                                cudaMemcpyDeviceToHost, e->stream));
+    off += e->n[c];
+  }
+  EN_CUDA(cudaStreamSynchronize(e->stream));
   return NBODY_OK;
 }
 
@@ -458,14 +517,12 @@ nbody_status use_kernel(nbody_ensemble* e, const EnsKernel* k) {
 }
 
 nbody_status launch_ens_pack(nbody_ensemble* e) {
+  if (e->fmt == kRecRel && !e->sorted)  // tile-relative: bodies into Morton order first
+    EN_TRY(ens_reorder_state(e, e->stream));
   ens_pack_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
       e->L, e->cid, e->X, e->V, e->M, e->jb64, e->fmt == kRecX2 ? e->jbx : nullptr);
   EN_CUDA(cudaGetLastError());
-  if (e->fmt == kRecRel) {
-    EN_TRY(ens_order(e, e->stream));
-    e->since_sort = 0;
-    EN_TRY(ens_tiles(e, e->stream));
-  }
+  if (e->fmt == kRecRel) EN_TRY(ens_tiles(e, e->stream));
   return NBODY_OK;
 }
 
@@ -525,10 +582,15 @@ nbody_status ens_build_graph(nbody_ensemble* e) {
     return nbody_set_error(NBODY_ERR_CUDA, "instantiate: %s", cudaGetErrorString(ce));
   }
   if (e->fmt == kRecRel && !e->order_graph) {
+    const bool sorted = e->sorted, permuted = e->permuted;
+    const int since = e->since_sort;
     EN_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-    s = ens_order(e, e->stream);
+    s = ens_reorder_state(e, e->stream);
     g = nullptr;
     ce = cudaStreamEndCapture(e->stream, &g);
+    e->sorted = sorted;  // capturing ran nothing
+    e->permuted = permuted;
+    e->since_sort = since;
     if (s != NBODY_OK) {
       if (g) cudaGraphDestroy(g);
       return s;
@@ -556,7 +618,7 @@ nbody_status ens_autotune(nbody_ensemble* e) {
   const EnsKernel* best_k = e->kern;
   int best_tpi = 8;
   for (const EnsKernel& k : ens_registry()) {
-    if (k.precision != e->precision || k.fmt != e->fmt) continue;
+    if (k.precision != e->precision || k.fmt != e->fmt || (k.fmt == kRecRel && k.near != e->near)) continue;
     EN_TRY(use_kernel(e, &k));
     if (e->fmt == kRecRel) EN_TRY(ens_tiles(e, e->stream));  // this kernel's tile size
     for (int j_per_item : {256, 512, 1024, 2048, 4096, 8192}) {
@@ -607,7 +669,7 @@ nbody_status nbody_ensemble_destroy(nbody_ensemble* e) {
     if (ev) cudaEventDestroy(ev);
   void* bufs[] = {e->state, e->P, e->jb64, e->jbx, e->cid, e->cl, e->items, e->counter,
                   e->status, e->blk_cluster, e->blk_row, e->phi, e->Tc, e->Uc,
-                  e->seg, e->bbox, e->sort_keys, e->sort_idx, e->sort_tmp};
+                  e->seg, e->bbox, e->sort_keys, e->sort_idx, e->sort_tmp, e->perm, e->scratch};
   for (void* p : bufs) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -623,11 +685,13 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
   if (cfg->precision != NBODY_FP64 && cfg->precision != NBODY_MIXED)
     return nbody_set_error(NBODY_ERR_INVALID_ARG, "precision = %d", cfg->precision);
   if (cfg->tiles_per_item < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "tiles_per_item < 0");
-  if (cfg->precision == NBODY_MIXED && cfg->pair_variant != 0 && cfg->pair_variant != 3)
+  if (cfg->precision == NBODY_MIXED && cfg->pair_variant != 0 && cfg->pair_variant != 3 &&
+      cfg->pair_variant != 5)
     return nbody_set_error(NBODY_ERR_INVALID_ARG,
-                           "ensemble pair_variant = %d (0 tile-relative, 3 packed hi/lo)", cfg->pair_variant);
+                           "ensemble pair_variant = %d (0 near/far tile-relative, 3 packed hi/lo, "
+                           "5 plain tile-relative)", cfg->pair_variant);
   if (cfg->sort_every < 0) return nbody_set_error(NBODY_ERR_INVALID_ARG, "sort_every < 0");
-  const bool rel = cfg->precision == NBODY_MIXED && cfg->pair_variant == 0;
+  const bool rel = cfg->precision == NBODY_MIXED && (cfg->pair_variant == 0 || cfg->pair_variant == 5);
   if (rel && C > 65536)
     return nbody_set_error(NBODY_ERR_INVALID_ARG,
                            "tile-relative ensembles hold at most 65536 clusters (use pair_variant 3)");
@@ -659,6 +723,7 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
   e->dev = cfg->device;
   e->precision = cfg->precision;
   e->fmt = cfg->precision == NBODY_FP64 ? kRecF64 : (rel ? kRecRel : kRecX2);
+  e->near = cfg->pair_variant == 5 ? 0 : 1;
   e->sort_every = cfg->sort_every > 0 ? cfg->sort_every : 16;
   while ((1LL << (e->sort_bits - 48)) < C) ++e->sort_bits;  // cluster id above the 48-bit code
   cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->dev);
@@ -692,7 +757,8 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     raw->M = raw->state + 6 * Ls;
     raw->D = raw->state + 7 * Ls;
     EN_CUDA(cudaMalloc(&raw->jb64, sizeof(JBody64) * Ls));
-    if (raw->precision == NBODY_MIXED) EN_CUDA(cudaMalloc(&raw->jbx, sizeof(JBodyX2) * Ls));
+    // JBodyX2 records, or tiles of TJ + 1 JBodyNF records (TJ >= 64)
+    if (raw->precision == NBODY_MIXED) EN_CUDA(cudaMalloc(&raw->jbx, sizeof(JBodyNF) * (Ls / 64) * 65));
     EN_CUDA(cudaMalloc(&raw->cid, sizeof(int) * Ls));
     EN_CUDA(cudaMemcpy(raw->cid, cid.data(), sizeof(int) * Ls, cudaMemcpyHostToDevice));
     EN_CUDA(cudaMalloc(&raw->cl, sizeof(ClusterDev) * raw->C));
@@ -707,12 +773,15 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     EN_CUDA(cudaMalloc(&raw->Tc, sizeof(double) * raw->C));
     EN_CUDA(cudaMalloc(&raw->Uc, sizeof(double) * raw->C));
     if (raw->fmt == kRecRel) {
-      static_assert(sizeof(JBodyX2) >= sizeof(JBodyRel) * 65 / 64, "jbx holds tiles of >= 64");
       EN_CUDA(cudaMalloc(&raw->seg, sizeof(int) * Ls));
       EN_CUDA(cudaMemcpy(raw->seg, seg.data(), sizeof(int) * Ls, cudaMemcpyHostToDevice));
       EN_CUDA(cudaMalloc(&raw->bbox, sizeof(double) * 6 * raw->C));
       EN_CUDA(cudaMalloc(&raw->sort_keys, sizeof(uint64_t) * 2 * Ls));
       EN_CUDA(cudaMalloc(&raw->sort_idx, sizeof(int) * 2 * Ls));
+      EN_CUDA(cudaMalloc(&raw->perm, sizeof(int) * 2 * Ls));
+      iota_kernel<<<(raw->L + kBlock - 1) / kBlock, kBlock, 0, raw->stream>>>(raw->L, raw->perm);
+      EN_CUDA(cudaGetLastError());
+      EN_CUDA(cudaMalloc(&raw->scratch, sizeof(double) * 13 * Ls));
       EN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, raw->sort_tmp_bytes, raw->sort_keys,
                                               raw->sort_keys + Ls, raw->sort_idx,
                                               raw->sort_idx + Ls, raw->L, 0, raw->sort_bits,
@@ -721,7 +790,7 @@ nbody_status nbody_ensemble_create(nbody_ensemble** out, const nbody_ensemble_co
     }
     for (auto& ev : raw->ev) EN_CUDA(cudaEventCreate(&ev));
     for (const EnsKernel& k : ens_registry())
-      if (k.precision == raw->precision && k.fmt == raw->fmt) {
+      if (k.precision == raw->precision && k.fmt == raw->fmt && (k.fmt != kRecRel || k.near == raw->near)) {
         EN_TRY(use_kernel(raw, &k));
         break;
       }
@@ -754,6 +823,11 @@ nbody_status nbody_ensemble_set_state(nbody_ensemble* e, const double* x, const 
     off += e->n[c];
   }
   EN_CUDA(cudaMemsetAsync(e->D, 0, sizeof(double) * 6 * L, e->stream));
+  if (e->perm) {  // the caller's order again; re-ordered before the next evaluation
+    iota_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(e->L, e->perm);
+    EN_CUDA(cudaGetLastError());
+  }
+  e->sorted = e->permuted = false;
   EN_TRY(launch_ens_pack(e));
   EN_CUDA(cudaStreamSynchronize(e->stream));
   e->have_derivs = false;
@@ -765,18 +839,8 @@ nbody_status nbody_ensemble_set_state(nbody_ensemble* e, const double* x, const 
 nbody_status nbody_ensemble_get_state(nbody_ensemble* e, double* x, double* y, double* z,
                                       double* vx, double* vy, double* vz) {
   EN_TRY(ens_check(e));
-  const size_t L = e->L;
   double* dst[6] = {x, y, z, vx, vy, vz};
-  const double* src[6] = {e->X, e->X + L, e->X + 2 * L, e->V, e->V + L, e->V + 2 * L};
-  long long off = 0;
-  for (int c = 0; c < e->C; ++c) {
-    for (int k = 0; k < 6; ++k)
-      if (dst[k])
-        EN_CUDA(cudaMemcpyAsync(dst[k] + off, src[k] + e->row0[c], sizeof(double) * e->n[c],
-                                cudaMemcpyDeviceToHost, e->stream));
-    off += e->n[c];
-  }
-  EN_CUDA(cudaStreamSynchronize(e->stream));
+  EN_TRY(ens_download(e, e->X, dst, 6));  // X(3) and V(3) are consecutive state arrays
   return ens_status(e);
 }
 
@@ -784,17 +848,8 @@ nbody_status nbody_ensemble_get_derivs(nbody_ensemble* e, double* ax, double* ay
                                        double* jx, double* jy, double* jz) {
   EN_TRY(ens_check(e));
   if (!e->have_derivs) return nbody_set_error(NBODY_ERR_STATE, "no derivatives yet");
-  const size_t L = e->L;
   double* dst[6] = {ax, ay, az, jx, jy, jz};
-  long long off = 0;
-  for (int c = 0; c < e->C; ++c) {
-    for (int k = 0; k < 6; ++k)
-      if (dst[k])
-        EN_CUDA(cudaMemcpyAsync(dst[k] + off, e->D + k * L + e->row0[c], sizeof(double) * e->n[c],
-                                cudaMemcpyDeviceToHost, e->stream));
-    off += e->n[c];
-  }
-  EN_CUDA(cudaStreamSynchronize(e->stream));
+  EN_TRY(ens_download(e, e->D, dst, 6));
   return ens_status(e);
 }
 

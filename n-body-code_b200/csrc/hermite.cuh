@@ -238,15 +238,28 @@ static __global__ void correct_kernel(int n, int ld, int S, const double* __rest
 }
 
 // out[c][i] = sum_s P[s][c][i] for rows [i_begin, i_end), splits in order.
+// With a status word (callers that cannot read it back before using the
+// outputs), a non-zero word - a pair kernel gave up a bounded wait - makes
+// every output NaN instead.  With an index map, row i is written to
+// out[c][index[i]] (partials kept in Morton order, outputs in the caller's
+// body order).
 static __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int S,
-                                     const double* __restrict__ P, SoA6 out) {
+                                     const double* __restrict__ P, SoA6 out,
+                                     const int* __restrict__ status = nullptr,
+                                     const int* __restrict__ index = nullptr) {
   const int i = i_begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= i_end) return;
   double* dst[6] = {out.ax, out.ay, out.az, out.jx, out.jy, out.jz};
+  const int o = index ? index[i] : i;
+  if (status && *status != 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) dst[c][o] = __longlong_as_double(0x7FF8000000000000ll);
+    return;
+  }
   double sum[6];
   split_sums(P, ld, S, i, sum);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) dst[c][i] = sum[c];
+  for (int c = 0; c < 6; ++c) dst[c][o] = sum[c];
 }
 
 // Initial step criterion min_i eta0 |a| / |j| (published via ctl).

@@ -12,15 +12,23 @@
 // Scratch lives in one file-scope __device__ array (g_scratch, 16 MiB): the
 // j-records of the packed input, the split-j partial sums, and a status word.
 // Every GPU that loads this library holds those 16 MiB until the process
-// exits.  Host code cannot use the symbol g_scratch as a device address, so
-// the first call on each device (with that device current) looks the address
-// up with cudaGetSymbolAddress and caches it; make that first call before any
-// stream capture.  All calls share the array and it keeps the last call's
-// contents: each call rewrites every byte it reads (the j-records up to the
-// padded size, every split slice of the partial sums) and clears the status
-// word first.  Calls whose work overlaps on the GPU (different streams, no
-// ordering between them) race on the array and corrupt each other's results;
-// order them on one stream or serialise them.
+// exits.  Host code cannot use the symbol g_scratch as a device address: each
+// call whose stream is not capturing looks the address up again with
+// cudaGetSymbolAddress, with the caller's device current (so a context that
+// was reset and rebuilt, which may place the array elsewhere, is never
+// written through a stale address); a call on a capturing stream uses the
+// address of the last such lookup on that device, so the first call on a
+// device must come before any stream capture.  All calls share the array and
+// it keeps the last call's contents: each call rewrites every byte it reads
+// (the j-records up to the padded size, every split slice of the partial
+// sums) and clears the status word first.  Calls whose work overlaps on the
+// GPU (different streams, no ordering between them) race on the array and
+// corrupt each other's results; order them on one stream or serialise them.
+//
+// The call returns without waiting for the GPU, so it cannot report a
+// bounded-wait timeout of its pair kernel as a status: the split reduction
+// reads the status word instead and then writes NaN to every output, which
+// the caller sees in its results.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,7 +57,7 @@ __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 struct DeviceSetup {
   bool ready = false;
-  unsigned char* base = nullptr;  // device address of g_scratch on this device
+  unsigned char* base = nullptr;  // device address of g_scratch from the last lookup
   int sms = 0;
   int occ_fp64 = 1, occ_mixed = 1;
 };
@@ -58,36 +66,72 @@ DeviceSetup g_dev[kMaxDevices];
 
 constexpr int kIptFp64 = 2, kIptMixed = 4;
 const void* kernel_fp64() { return reinterpret_cast<const void*>(&pair_fp64_kernel<kThreads, kIptFp64, kTile>); }
-// the engine's default mixed kernel (packed pairs), so both entry points do identical arithmetic
+// the packed hi/lo kernel with FP64 accumulators in registers (the engine's
+// pair_variant 2 at this shape), so both entry points do identical arithmetic
 const void* kernel_mixed() { return reinterpret_cast<const void*>(&pair_mixed_x2_kernel<kThreads, kIptMixed, kTile>); }
 
-nbody_status setup(int dev, DeviceSetup** out) {
+// Device set-up (once) and the scratch address (looked up on every call whose
+// stream is not capturing).  Errors made here are this call's own: the entry
+// point has checked that none was pending before it.
+nbody_status setup(int dev, cudaStream_t cs, DeviceSetup** out) {
   std::lock_guard<std::mutex> g(g_mu);
   DeviceSetup& d = g_dev[dev];
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(cs, &cap) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cap = cudaStreamCaptureStatusActive;  // treat an unanswerable stream as capturing
+  }
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
   if (!d.ready) {
+    if (capturing)
+      return nbody_set_error(NBODY_ERR_STATE,
+                             "nbody_acc_jerk_noalloc: the first call on device %d came during a "
+                             "stream capture; make one call before capturing",
+                             dev);
     int major = 0;
-    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+        major != 10) {
+      (void)cudaGetLastError();
       return nbody_set_error(NBODY_ERR_NO_DEVICE, "nbody_acc_jerk_noalloc: device %d is not sm_100", dev);
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: cudaGetSymbolAddress: %s",
-                             cudaGetErrorString(e));
-    cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        d.sms < 1) {
+      (void)cudaGetLastError();
+      return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: SM count of device %d", dev);
+    }
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_fp64, kernel_fp64(), kThreads,
                                                       2 * kTile * sizeof(JBody64)) != cudaSuccess ||
-        d.occ_fp64 < 1)
-      d.occ_fp64 = 1;
+        d.occ_fp64 < 1) {
+      (void)cudaGetLastError();
+      d.occ_fp64 = 1;  // only sizes the j-split
+    }
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_mixed, kernel_mixed(), kThreads,
                                                       2 * kTile * sizeof(JBodyX2)) != cudaSuccess ||
-        d.occ_mixed < 1)
+        d.occ_mixed < 1) {
+      (void)cudaGetLastError();
       d.occ_mixed = 1;
-    cudaGetLastError();
+    }
+  }
+  if (!capturing) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      (void)cudaGetLastError();
+      return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: cudaGetSymbolAddress: %s",
+                             cudaGetErrorString(e));
+    }
     d.base = static_cast<unsigned char*>(p);
     d.ready = true;
   }
   *out = &d;
   return NBODY_OK;
+}
+
+// This call's launch error, if any (none was pending when the call began).
+nbody_status launched(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return NBODY_OK;
+  return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: %s: %s", what, cudaGetErrorString(e));
 }
 
 }  // namespace
@@ -117,8 +161,17 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return nbody_set_error(NBODY_ERR_NO_DEVICE, "nbody_acc_jerk_noalloc: no current device");
+  // an error left pending by the caller's own earlier work stays theirs:
+  // report it without clearing it, and do not run on top of it
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return nbody_set_error(NBODY_ERR_CUDA,
+                           "nbody_acc_jerk_noalloc: a CUDA error was already pending in this "
+                           "thread (%s); nothing was launched and the error was left in place",
+                           cudaGetErrorString(pending));
+  cudaStream_t cs = static_cast<cudaStream_t>(stream);
   DeviceSetup* d = nullptr;
-  nbody_status st = setup(dev, &d);
+  nbody_status st = setup(dev, cs, &d);
   if (st != NBODY_OK) return st;
 
   const bool fp64 = precision == NBODY_FP64;
@@ -147,12 +200,14 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
     }
   }
 
-  cudaStream_t cs = static_cast<cudaStream_t>(stream);
-  if (cudaMemsetAsync(status, 0, sizeof(int), cs) != cudaSuccess)
+  if (cudaMemsetAsync(status, 0, sizeof(int), cs) != cudaSuccess) {
+    (void)cudaGetLastError();
     return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: clearing the status word failed");
+  }
   pack_kernel<<<(ld + 255) / 256, 256, 0, cs>>>(
       n, ld, SoA7{x, y, z, m, vx, vy, vz}, fp64 ? reinterpret_cast<JBody64*>(jb) : nullptr, nullptr,
       fp64 ? nullptr : reinterpret_cast<JBodyX2*>(jb));
+  if ((st = launched("pack_kernel launch")) != NBODY_OK) return st;
   PairArgs a;
   a.i_begin = 0;
   a.i_end = n;
@@ -170,9 +225,10 @@ extern "C" nbody_status nbody_acc_jerk_noalloc(int n, double eps2, int precision
   else
     pair_mixed_x2_kernel<kThreads, kIptMixed, kTile><<<grid, kThreads, 2 * kTile * sizeof(JBodyX2), cs>>>(
         reinterpret_cast<const JBodyX2*>(jb), a);
-  reduce_splits_kernel<<<(n + 255) / 256, 256, 0, cs>>>(0, n, ld, split, P, SoA6{ax, ay, az, jx, jy, jz});
-  const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess)
-    return nbody_set_error(NBODY_ERR_CUDA, "nbody_acc_jerk_noalloc: launch failed: %s", cudaGetErrorString(e));
+  if ((st = launched("pair kernel launch")) != NBODY_OK) return st;
+  // a pair-kernel timeout (status word set) turns every output into NaN
+  reduce_splits_kernel<<<(n + 255) / 256, 256, 0, cs>>>(0, n, ld, split, P,
+                                                        SoA6{ax, ay, az, jx, jy, jz}, status);
+  if ((st = launched("reduce_splits_kernel launch")) != NBODY_OK) return st;
   return NBODY_OK;
 }

@@ -29,9 +29,11 @@
 //          accuracy however close two bodies are), velocities and the rest
 //          of the pair math in float with the MUFU rsqrt, float partial sums
 //          over one j-tile flushed into double accumulators after each tile.
-//   Mixed, tile-relative (default): the same pair math on separations formed
-//          from per-tile float offsets (RowsMixedRel below): one add per
-//          component instead of three.
+//   Mixed, near/far tile-relative (default for large systems): bodies in
+//          Morton order, j-tiles of float offsets from each tile's centre;
+//          the separation costs one add per component for tiles far from a
+//          warp's rows and is formed in double-single for near tiles
+//          (RowsMixedNF below), so close pairs keep the hi/lo accuracy.
 #pragma once
 #include <cstdint>
 
@@ -65,20 +67,39 @@ struct __align__(16) JBodyX2 {
   float2 vy, vz, pad0, pad1;
 };
 
-// j-record, tile-relative packed mixed path: 64 bytes, every field twice.
-// A j-tile's first record is a header whose x, y, z hold the tile centre c
-// (m = 0); each body record holds -D(x) with D(x) = fl(fl(c - x_hi) - x_lo),
-// x_hi = fl(x), x_lo = fl(x - x_hi).  Tiles are built from bodies in Morton
-// order, so the offsets within a tile are small.
-struct __align__(16) JBodyRel {
+// j-record of the near/far tile-relative kernel: 96 bytes, every field twice.
+// Record 0 of a tile is its header: x, y, z = the tile centre c; m = (lo_x,
+// lo_y), vx = (lo_z, hi_x), vy = (hi_y, hi_z) = the tile's bounding box
+// (rounded outward to float); vz = (R, 0) with R >= max |x_j - c| over the
+// tile's bodies.  A body record holds x, y, z = -D_hi and xl, yl, zl = -D_lo,
+// where (D_hi, D_lo) = ds_offset(c, x_hi, x_lo) is the double-single value of
+// c - x, and its mass and velocity.
+struct __align__(16) JBodyNF {
   float2 x, y, z, m;
   float2 vx, vy, vz, pad;
+  float2 xl, yl, zl, pad2;
 };
 
-// FP64 source of the i-rows of the tile-relative kernel (body order).
+// FP64 source of the i-rows of the tile-relative kernels.
 struct RowSrc {
   const double *x, *y, *z, *vx, *vy, *vz;
 };
+
+// (hi, lo) with hi + lo = c - (xh + xl) to about 2^-48 relative: the exact
+// difference c - xh as a float sum s + e (Knuth's TwoSum), the low part xl
+// folded into e, and the result renormalised by a second TwoSum.  Every
+// operation rounds to nearest and none is contracted, so the records
+// (rel_tile_nf_kernel) and the i-rows (RowsMixedNF) get bit-identical
+// offsets for the same body and a pair's self term cancels exactly.
+__device__ __forceinline__ void ds_offset(float c, float xh, float xl, float& hi, float& lo) {
+  const float s = __fsub_rn(c, xh);
+  const float bb = __fsub_rn(s, c);
+  const float e = __fsub_rn(__fsub_rn(c, __fsub_rn(s, bb)), __fadd_rn(xh, bb));
+  const float t = __fsub_rn(e, xl);
+  hi = __fadd_rn(s, t);
+  const float b2 = __fsub_rn(hi, s);
+  lo = __fadd_rn(__fsub_rn(s, __fsub_rn(hi, b2)), __fsub_rn(t, b2));
+}
 
 // Packed single precision (sm_100+): one instruction performs the operation
 // on both halves of a 64-bit register pair.  Same FP32-pipe throughput per
@@ -474,53 +495,148 @@ struct RowsMixedX2 {
   }
 };
 
-// Tile-relative rows.  With c the tile centre and D(x) = fl(fl(c - x_hi) -
-// x_lo), r_ij = D(x_i) - D(x_j): the record holds -D(x_j), the row forms
-// D(x_i) once per tile.  A pair then costs one add per component instead of
-// the three of the hi/lo form (25 instead of 31 FP32 lane-ops).  The self
-// pair cancels exactly; otherwise the error of r_ij is about one float ulp
-// of |x_i - c| + |x_j - c|: for the close pairs that dominate a body's
-// force both offsets are of the order of the tile's radius, which Morton
-// ordering keeps near the local interparticle spacing.
-template <int NT_, int IPT, int TJ_, int ACC_SMEM, int JU>
-struct RowsMixedRel : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
-  using Base = RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU>;
-  using JB = JBodyRel;
-  static constexpr int NP = Base::NP, NT = NT_, TJ = TJ_;
+// The pair terms shared by the packed mixed kernels once the separation
+// (dx, dy, dz) of rows (2p, 2p+1) is formed: mj = (m_j, m_j), the j-body's
+// velocity, and the accumulators of this tile.
+template <int NP>
+__device__ __forceinline__ void pair_terms_x2(int p, uint64_t dx, uint64_t dy, uint64_t dz,
+                                              uint64_t mj, uint64_t vxj, uint64_t vyj,
+                                              uint64_t vzj, const uint64_t* ui, const uint64_t* vi,
+                                              const uint64_t* wi, uint64_t eps2, uint64_t m3,
+                                              uint64_t* fax, uint64_t* fay, uint64_t* faz,
+                                              uint64_t* fjx, uint64_t* fjy, uint64_t* fjz) {
+  const uint64_t du = f2_sub(vxj, ui[p]);
+  const uint64_t dv = f2_sub(vyj, vi[p]);
+  const uint64_t dw = f2_sub(vzj, wi[p]);
+  const uint64_t s = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, eps2)));
+  const uint64_t rv = f2_fma(dx, du, f2_fma(dy, dv, f2_mul(dz, dw)));
+  float s0, s1;
+  f2_unpack(s, s0, s1);
+  const uint64_t y = f2_pack(rsqrt_mufu(s0), rsqrt_mufu(s1));
+  const uint64_t y2 = f2_pack(rcp_mufu(s0), rcp_mufu(s1));
+  const uint64_t q = f2_mul(mj, f2_mul(y, y2));
+  const uint64_t c = f2_mul(rv, f2_mul(y2, m3));
+  fax[p] = f2_fma(q, dx, fax[p]);
+  fay[p] = f2_fma(q, dy, fay[p]);
+  faz[p] = f2_fma(q, dz, faz[p]);
+  fjx[p] = f2_fma(q, f2_fma(c, dx, du), fjx[p]);
+  fjy[p] = f2_fma(q, f2_fma(c, dy, dv), fjy[p]);
+  fjz[p] = f2_fma(q, f2_fma(c, dz, dw), fjz[p]);
+}
 
-  // Rows row, row + NT, ... read (clamped to row_max) from the FP64 source.
-  __device__ __forceinline__ void begin_rows(const RowSrc& src, int row, int row_max, double e2,
-                                             unsigned char* extra) {
+// Near/far tile-relative rows (the default mixed kernel for large systems).
+// The engine keeps its bodies in Morton order, and each warp takes 32 * IPT
+// consecutive positions (row k of lane l is warp_row0 + 32 k + l), so a
+// warp's rows occupy a compact region, whose bounding box begin_rows records.
+// Each j-tile is then classified per warp (a warp-uniform branch):
+//   far  - the boxes are separated by d > 0 with d >= R / 2 (R: the tile's
+//          largest offset from its centre).  r_ij = D(x_i) + (-D_hi(x_j)) with
+//          D(x_i) = fl(fl(c - x_hi) - x_lo): one add per component.  Its error
+//          is at most about 2^-24 (3 |r| + 3 R) <= 9 * 2^-24 |r|, float
+//          accuracy of the separation itself.
+//   near - everything else (the warp's own tiles, its neighbours, and tiles
+//          whose box straddles a jump of the Morton curve): the separation in
+//          double-single, r = (D_hi(x_i) - D_hi(x_j)) + (D_lo(x_i) - D_lo(x_j))
+//          with (D_hi, D_lo) = ds_offset(c, x_hi, x_lo), three adds per
+//          component like the hi/lo kernel, so close pairs keep float
+//          relative accuracy however close they are, and the self pair
+//          cancels exactly.
+// NEAR = 0 takes the far form for every tile (the plain tile-relative
+// kernel, kept as a measured comparison).
+template <int NT_, int IPT, int TJ_, int ACC_SMEM, int JU, int NEAR>
+struct RowsMixedNF : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
+  using Base = RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU>;
+  using JB = JBodyNF;
+  static constexpr int NP = Base::NP, NT = NT_, TJ = TJ_, kNear = NEAR;
+  static constexpr size_t kExtraSmem = Base::kExtraSmem;
+  float blo[3], bhi[3];  // bounding box of the warp's rows (same in every lane)
+  int warp_row0;         // first row of this warp
+  int near_tiles;
+
+  __device__ __forceinline__ int row_of(int k) const { return warp_row0 + 32 * k + (threadIdx.x & 31); }
+
+  // Rows of the CTA starting at cta_row0, read (clamped to row_max) from the
+  // FP64 source; rows >= row_end are padding and stay out of the box.
+  __device__ __forceinline__ void begin_rows(const RowSrc& src, int cta_row0, int row_max,
+                                             int row_end, double e2, unsigned char* extra) {
     auto hl = [](double v, float& h, float& l) {
       h = static_cast<float>(v);
       l = static_cast<float>(v - static_cast<double>(h));
     };
+    warp_row0 = cta_row0 + (threadIdx.x >> 5) * 32 * IPT;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      const int i0 = min(row + (2 * p) * NT, row_max), i1 = min(row + (2 * p + 1) * NT, row_max);
+      const int r0 = row_of(2 * p), r1 = row_of(2 * p + 1);
+      const int i0 = min(r0, row_max), i1 = min(r1, row_max);
+      const double x0[3] = {src.x[i0], src.y[i0], src.z[i0]};
+      const double x1[3] = {src.x[i1], src.y[i1], src.z[i1]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (r0 < row_end) { lo[k] = fmin(lo[k], x0[k]); hi[k] = fmax(hi[k], x0[k]); }
+        if (r1 < row_end) { lo[k] = fmin(lo[k], x1[k]); hi[k] = fmax(hi[k], x1[k]); }
+      }
       float h0, l0, h1, l1;
-      hl(src.x[i0], h0, l0); hl(src.x[i1], h1, l1);
+      hl(x0[0], h0, l0); hl(x1[0], h1, l1);
       this->xh[p] = f2_pack(h0, h1); this->xl[p] = f2_pack(l0, l1);
-      hl(src.y[i0], h0, l0); hl(src.y[i1], h1, l1);
+      hl(x0[1], h0, l0); hl(x1[1], h1, l1);
       this->yh[p] = f2_pack(h0, h1); this->yl[p] = f2_pack(l0, l1);
-      hl(src.z[i0], h0, l0); hl(src.z[i1], h1, l1);
+      hl(x0[2], h0, l0); hl(x1[2], h1, l1);
       this->zh[p] = f2_pack(h0, h1); this->zl[p] = f2_pack(l0, l1);
       this->ui[p] = f2_pack(static_cast<float>(src.vx[i0]), static_cast<float>(src.vx[i1]));
       this->vi[p] = f2_pack(static_cast<float>(src.vy[i0]), static_cast<float>(src.vy[i1]));
       this->wi[p] = f2_pack(static_cast<float>(src.vz[i0]), static_cast<float>(src.vz[i1]));
     }
+    // the warp's box, rounded outward to float (no valid row: +inf/-inf,
+    // which every tile is far from)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float l = __double2float_rd(lo[k]), h = __double2float_ru(hi[k]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        l = fminf(l, __shfl_xor_sync(0xffffffffu, l, o));
+        h = fmaxf(h, __shfl_xor_sync(0xffffffffu, h, o));
+      }
+      blo[k] = l;
+      bhi[k] = h;
+    }
+    near_tiles = 0;
     this->init_acc(e2, extra);
   }
 
+  // Far: the boxes are apart by d > 0 with d^2 >= R^2 / 4.  The gaps are
+  // computed from float boxes rounded outward, so d never exceeds the true
+  // distance between any row and any body of the tile.
+  __device__ __forceinline__ bool is_far(const JBodyNF& h) const {
+    const float tlo[3] = {h.m.x, h.m.y, h.vx.x}, thi[3] = {h.vx.y, h.vy.x, h.vy.y};
+    float d2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float g = fmaxf(0.f, fmaxf(__fsub_rd(blo[k], thi[k]), __fsub_rd(tlo[k], bhi[k])));
+      d2 = __fmaf_rd(g, g, d2);
+    }
+    const float R = h.vz.x;
+    return d2 > 0.f && d2 >= __fmul_ru(0.25f, __fmul_ru(R, R));
+  }
+
   __device__ __forceinline__ void consume(const JB* tile) {
-    const ulonglong2* hd = reinterpret_cast<const ulonglong2*>(tile);
-    const ulonglong2 c0 = hd[0], c1 = hd[1];  // (cx, cy), (cz, 0)
-    uint64_t ox[NP], oy[NP], oz[NP];           // D(x_i)
+    const JBodyNF& h = tile[0];
+    if (!NEAR || is_far(h)) {
+      consume_far(tile, h);
+    } else {
+      ++near_tiles;
+      consume_near(tile, h);
+    }
+  }
+
+  __device__ __forceinline__ void consume_far(const JB* tile, const JBodyNF& h) {
+    const uint64_t cx = f2_pack(h.x.x, h.x.x), cy = f2_pack(h.y.x, h.y.x), cz = f2_pack(h.z.x, h.z.x);
+    uint64_t ox[NP], oy[NP], oz[NP];  // D(x_i) to float accuracy: fl(fl(c - x_hi) - x_lo)
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      ox[p] = f2_sub(f2_sub(c0.x, this->xh[p]), this->xl[p]);
-      oy[p] = f2_sub(f2_sub(c0.y, this->yh[p]), this->yl[p]);
-      oz[p] = f2_sub(f2_sub(c1.x, this->zh[p]), this->zl[p]);
+      ox[p] = f2_sub(f2_sub(cx, this->xh[p]), this->xl[p]);
+      oy[p] = f2_sub(f2_sub(cy, this->yh[p]), this->yl[p]);
+      oz[p] = f2_sub(f2_sub(cz, this->zh[p]), this->zl[p]);
     }
     uint64_t fax[NP], fay[NP], faz[NP], fjx[NP], fjy[NP], fjz[NP];
 #pragma unroll
@@ -532,33 +648,81 @@ struct RowsMixedRel : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
       const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
       // r0 = (-Dx, -Dy) r1 = (-Dz, m) r2 = (vx, vy) r3 = (vz, pad)
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
-        const uint64_t dx = f2_add(r0.x, ox[p]);
-        const uint64_t dy = f2_add(r0.y, oy[p]);
-        const uint64_t dz = f2_add(r1.x, oz[p]);
-        const uint64_t du = f2_sub(r2.x, this->ui[p]);
-        const uint64_t dv = f2_sub(r2.y, this->vi[p]);
-        const uint64_t dw = f2_sub(r3.x, this->wi[p]);
-        const uint64_t s = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, eps2)));
-        const uint64_t rv = f2_fma(dx, du, f2_fma(dy, dv, f2_mul(dz, dw)));
-        float s0, s1;
-        f2_unpack(s, s0, s1);
-        const uint64_t y = f2_pack(rsqrt_mufu(s0), rsqrt_mufu(s1));
-        const uint64_t y2 = f2_pack(rcp_mufu(s0), rcp_mufu(s1));
-        const uint64_t q = f2_mul(r1.y, f2_mul(y, y2));
-        const uint64_t c = f2_mul(rv, f2_mul(y2, m3));
-        fax[p] = f2_fma(q, dx, fax[p]);
-        fay[p] = f2_fma(q, dy, fay[p]);
-        faz[p] = f2_fma(q, dz, faz[p]);
-        fjx[p] = f2_fma(q, f2_fma(c, dx, du), fjx[p]);
-        fjy[p] = f2_fma(q, f2_fma(c, dy, dv), fjy[p]);
-        fjz[p] = f2_fma(q, f2_fma(c, dz, dw), fjz[p]);
+      for (int p = 0; p < NP; ++p)
+        pair_terms_x2<NP>(p, f2_add(r0.x, ox[p]), f2_add(r0.y, oy[p]), f2_add(r1.x, oz[p]), r1.y,
+                          r2.x, r2.y, r3.x, this->ui, this->vi, this->wi, eps2, m3, fax, fay, faz,
+                          fjx, fjy, fjz);
+    }
+    flush_all(fax, fay, faz, fjx, fjy, fjz);
+  }
+
+  __device__ __forceinline__ void consume_near(const JB* tile, const JBodyNF& h) {
+    const float c[3] = {h.x.x, h.y.x, h.z.x};
+    uint64_t oh[3][NP], ol[3][NP];  // (D_hi, D_lo)(x_i), bit-identical to the records'
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const uint64_t xs[3] = {this->xh[p], this->yh[p], this->zh[p]};
+      const uint64_t ls[3] = {this->xl[p], this->yl[p], this->zl[p]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        float h0, h1, l0, l1, dh0, dl0, dh1, dl1;
+        f2_unpack(xs[k], h0, h1);
+        f2_unpack(ls[k], l0, l1);
+        ds_offset(c[k], h0, l0, dh0, dl0);
+        ds_offset(c[k], h1, l1, dh1, dl1);
+        oh[k][p] = f2_pack(dh0, dh1);
+        ol[k][p] = f2_pack(dl0, dl1);
       }
     }
+    uint64_t fax[NP], fay[NP], faz[NP], fjx[NP], fjy[NP], fjz[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) fax[p] = fay[p] = faz[p] = fjx[p] = fjy[p] = fjz[p] = 0ull;
+    const uint64_t eps2 = this->eps2, m3 = this->m3;
+#pragma unroll 1
+    for (int j = 1; j <= TJ; ++j) {
+      const ulonglong2* r = reinterpret_cast<const ulonglong2*>(tile + j);
+      const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];
+      // r4 = (-Dx_lo, -Dy_lo) r5 = (-Dz_lo, pad)
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        pair_terms_x2<NP>(p, f2_add(f2_add(r0.x, oh[0][p]), f2_add(r4.x, ol[0][p])),
+                          f2_add(f2_add(r0.y, oh[1][p]), f2_add(r4.y, ol[1][p])),
+                          f2_add(f2_add(r1.x, oh[2][p]), f2_add(r5.x, ol[2][p])), r1.y, r2.x, r2.y,
+                          r3.x, this->ui, this->vi, this->wi, eps2, m3, fax, fay, faz, fjx, fjy,
+                          fjz);
+    }
+    flush_all(fax, fay, faz, fjx, fjy, fjz);
+  }
+
+  __device__ __forceinline__ void flush_all(const uint64_t* fax, const uint64_t* fay,
+                                            const uint64_t* faz, const uint64_t* fjx,
+                                            const uint64_t* fjy, const uint64_t* fjz) {
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
       this->flush(0, p, fax[p]); this->flush(1, p, fay[p]); this->flush(2, p, faz[p]);
       this->flush(3, p, fjx[p]); this->flush(4, p, fjy[p]); this->flush(5, p, fjz[p]);
+    }
+  }
+
+  // out[c*stride + i] for this thread's rows i = row_of(k) < row_end.
+  __device__ __forceinline__ void store(double* out, size_t stride, int row_end) const {
+    constexpr int NACC = Base::NACC;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      const int i = row_of(k);
+      if (i < row_end) {
+        if (ACC_SMEM) {
+#pragma unroll
+          for (int c = 0; c < 6; ++c) out[c * stride + i] = this->acc_sm[(c * IPT + k) * NT + threadIdx.x];
+        } else {
+          out[0 * stride + i] = this->ax[k % NACC];
+          out[1 * stride + i] = this->ay[k % NACC];
+          out[2 * stride + i] = this->az[k % NACC];
+          out[3 * stride + i] = this->jx[k % NACC];
+          out[4 * stride + i] = this->jy[k % NACC];
+          out[5 * stride + i] = this->jz[k % NACC];
+        }
+      }
     }
   }
 };
@@ -582,6 +746,7 @@ struct PairArgs {
   size_t stride;
   int* status;
   RowSrc rows;             // i-row source of the tile-relative kernel (else unused)
+  unsigned long long* near_count = nullptr;  // near/far kernel: += near tiles (nullable)
 };
 
 template <class R>
@@ -628,26 +793,32 @@ __global__ void __launch_bounds__(NT, MINB) pair_mixed_x2_kernel(const JBodyX2* 
   pair_system<RowsMixedX2<NT, IPT, TJ, ACC_SMEM, JU>>(jb, a, smem_raw, full);
 }
 
-// Tile-relative mixed kernel: tile t is TJ + 1 records at jt + t*(TJ + 1)
-// (header first); i-rows come from a.rows, clamped below a.n_rows_pad.
-template <int NT, int IPT, int TJ, int ACC_SMEM = 1, int JU = 1, int MINB = 1>
-__global__ void __launch_bounds__(NT, MINB) pair_mixed_rel_kernel(const JBodyRel* __restrict__ jt,
-                                                                  PairArgs a) {
+// Near/far tile-relative mixed kernel: tile t is TJ + 1 records at
+// jt + t*(TJ + 1) (header first); i-rows (engine positions, Morton order) come
+// from a.rows, clamped below a.n_rows_pad; rows >= a.i_end are not stored and
+// stay out of the warps' bounding boxes.
+template <int NT, int IPT, int TJ, int ACC_SMEM = 1, int JU = 1, int MINB = 1, int NEAR = 1>
+__global__ void __launch_bounds__(NT, MINB) pair_mixed_nf_kernel(const JBodyNF* __restrict__ jt,
+                                                                 PairArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[2];
-  using R = RowsMixedRel<NT, IPT, TJ, ACC_SMEM, JU>;
+  using R = RowsMixedNF<NT, IPT, TJ, ACC_SMEM, JU, NEAR>;
   constexpr int kRecs = TJ + 1;
-  TilePipe<JBodyRel, kRecs> pipe;
-  pipe.init(reinterpret_cast<JBodyRel*>(smem_raw), full);
-  const int row = a.i_begin + blockIdx.x * R::ROWS + threadIdx.x;
+  TilePipe<JBodyNF, kRecs> pipe;
+  pipe.init(reinterpret_cast<JBodyNF*>(smem_raw), full);
+  const int row0 = a.i_begin + blockIdx.x * R::ROWS;
   const int t_begin = blockIdx.y * a.tiles_per_split;
   const int nt = max(0, min(a.tiles_per_split, a.n_tiles - t_begin));
   R r;
-  r.begin_rows(a.rows, row, a.n_rows_pad - 1, a.eps2, smem_raw + 2 * kRecs * sizeof(JBodyRel));
+  r.begin_rows(a.rows, row0, a.n_rows_pad - 1, a.i_end, a.eps2,
+               smem_raw + 2 * kRecs * sizeof(JBodyNF));
   if (!pipe.run(jt + static_cast<size_t>(t_begin) * kRecs, nt, a.status,
-                [&](const JBodyRel* tile) { r.consume(tile); }))
+                [&](const JBodyNF* tile) { r.consume(tile); }))
     return;
-  r.store(a.out + static_cast<size_t>(blockIdx.y) * 6 * a.stride, a.stride, row, a.i_end);
+  r.store(a.out + static_cast<size_t>(blockIdx.y) * 6 * a.stride, a.stride, a.i_end);
+  // near tiles of this launch, counted per warp (the unit that classifies)
+  if (NEAR && a.near_count && (threadIdx.x & 31) == 0 && r.near_tiles)
+    atomicAdd(a.near_count, static_cast<unsigned long long>(r.near_tiles));
 }
 
 // ---------------------------------------------------------------------------
@@ -691,44 +862,36 @@ __device__ __forceinline__ void pair_ensemble(const typename R::JB* __restrict__
   }
 }
 
-// Tile-relative ensemble: tiles of TJ + 1 records over the whole padded
-// array (cluster segments are multiples of 256 rows, so a tile never spans
-// two clusters); i-rows from the FP64 state `rows` (padded row order).
+// Near/far tile-relative ensemble: tiles of TJ + 1 records over the whole
+// padded array (cluster segments are multiples of 256 rows, so a tile never
+// spans two clusters); i-rows from the FP64 state `rows`, whose bodies each
+// cluster keeps in Morton order within its segment.  R is a RowsMixedNF.
 template <class R>
-__device__ __forceinline__ void pair_ensemble_rel(const JBodyRel* __restrict__ jt,
-                                                  const EnsItem* __restrict__ items, int n_items,
-                                                  unsigned int* counter, double* P, int* status,
-                                                  const RowSrc& rows, unsigned char* smem,
-                                                  uint64_t* full, int* s_item) {
-  constexpr int kRecs = R::TJ + 1;
-  TilePipe<JBodyRel, kRecs> pipe;
-  pipe.init(reinterpret_cast<JBodyRel*>(smem), full);
-  for (;;) {
-    if (threadIdx.x == 0) *s_item = static_cast<int>(atomicAdd(counter, 1u));
-    __syncthreads();
-    const int k = *s_item;
-    __syncthreads();
-    if (k >= n_items) return;
-    const EnsItem it = items[k];
-    const int row = it.row0 + threadIdx.x;  // cluster-relative
-    const RowSrc src{rows.x + it.jrow0, rows.y + it.jrow0, rows.z + it.jrow0,
-                     rows.vx + it.jrow0, rows.vy + it.jrow0, rows.vz + it.jrow0};
-    R r;
-    r.begin_rows(src, row, it.ld - 1, it.eps2, smem + 2 * kRecs * sizeof(JBodyRel));
-    const JBodyRel* ct = jt + static_cast<size_t>(it.jrow0 / R::TJ + it.t_begin) * kRecs;
-    if (!pipe.run(ct, it.nt, status, [&](const JBodyRel* tile) { r.consume(tile); })) return;
-    r.store(P + it.out_off, static_cast<size_t>(it.ld), row, it.rows_end);
-  }
-}
-
-template <class R>
-__global__ void __launch_bounds__(R::NT) ensemble_pair_rel_kernel(
-    const JBodyRel* __restrict__ jt, const EnsItem* __restrict__ items, int n_items,
+__global__ void __launch_bounds__(R::NT) ensemble_pair_nf_kernel(
+    const JBodyNF* __restrict__ jt, const EnsItem* __restrict__ items, int n_items,
     unsigned int* counter, double* P, int* status, RowSrc rows) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[2];
   __shared__ int s_item;
-  pair_ensemble_rel<R>(jt, items, n_items, counter, P, status, rows, smem_raw, full, &s_item);
+  constexpr int kRecs = R::TJ + 1;
+  TilePipe<JBodyNF, kRecs> pipe;
+  pipe.init(reinterpret_cast<JBodyNF*>(smem_raw), full);
+  for (;;) {
+    if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+    __syncthreads();
+    const int k = s_item;
+    __syncthreads();
+    if (k >= n_items) return;
+    const EnsItem it = items[k];
+    const RowSrc src{rows.x + it.jrow0, rows.y + it.jrow0, rows.z + it.jrow0,
+                     rows.vx + it.jrow0, rows.vy + it.jrow0, rows.vz + it.jrow0};
+    R r;
+    r.begin_rows(src, it.row0, it.ld - 1, it.rows_end, it.eps2,
+                 smem_raw + 2 * kRecs * sizeof(JBodyNF));
+    const JBodyNF* ct = jt + static_cast<size_t>(it.jrow0 / R::TJ + it.t_begin) * kRecs;
+    if (!pipe.run(ct, it.nt, status, [&](const JBodyNF* tile) { r.consume(tile); })) return;
+    r.store(P + it.out_off, static_cast<size_t>(it.ld), it.rows_end);
+  }
 }
 
 template <class R>

@@ -1,14 +1,18 @@
-// j-records of the tile-relative mixed kernel (JBodyRel, pair.cuh).
+// Morton ordering and the j-records of the near/far tile-relative mixed
+// kernel (JBodyNF, pair.cuh).
 //
-// Bodies are ordered along a Morton (Z-order) curve of their positions so
-// that each j-tile of TJ consecutive records covers a compact region; every
-// tile then stores its bodies as float offsets from the tile's centre.
+// Bodies are ordered along a Morton (Z-order) curve of their positions; the
+// engine keeps its state in that order (re-ordered every sort_every steps),
+// so each j-tile of TJ consecutive positions covers a compact region and
+// stores its bodies as offsets from the tile's centre.
 //
 //   bbox_partial_kernel   per-CTA min/max of x, y, z          (O(N) read, 24 B/body)
 //   morton_key_kernel     48-bit key (16 bits per axis) + index (O(N), 24 B in, 12 B out)
 //   (stable radix sort of (key, index) pairs: cub::DeviceRadixSort)
-//   rel_tile_kernel<TJ>   gather by sorted index, median tile centre, records
-//                         (O(N), 56 B gathered, 64 B written per body)
+//   gather_rows_kernel    the state (13 arrays) or a caller's input into that order
+//   scatter_rows_kernel   back to the caller's order (downloads, outputs)
+//   rel_tile_nf_kernel<TJ> tile box, centre and radius; hi/lo offsets per body
+//                         (O(N), 56 B read coalesced, 96 B written per body)
 //
 // Every step is deterministic: the bounding box reduces in a fixed order and
 // the sort is stable, so the records (and the pair sums) are reproducible.
@@ -107,79 +111,139 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
   vals[i] = i;
 }
 
-// Tile t (CTA t, TJ threads) = header + the bodies order[t*TJ + k], k < TJ
-// (slots >= n, and rows with cid[row] < 0 when cid is given, are zero-mass
-// padding at the centre).
-//
-// Centre c = the per-axis median of up to 32 evenly spaced bodies of the
-// tile, rounded to float (a tile that straddles a jump of the Morton curve
-// keeps its centre with the majority of its bodies).  The valid slots of a
-// tile are a prefix (padding sorts last), so the samples are slots
-// floor(j * nv / 32); warp 0 ranks them with shuffles.  A body's stored offset is -D, with
-// D = fl(fl(c - x_hi) - x_lo) the very float operations the pair kernel
-// applies to an i-row (x_hi = fl(x), x_lo = fl(x - x_hi)); the self pair
-// therefore cancels exactly (r_ii = -D + D = 0), whatever the rounding.
+
+// Records of the near/far kernel from bodies already in Morton order: tile t
+// (CTA t, TJ threads) = header + the bodies at positions t*TJ + k, k < TJ, read
+// straight (coalesced) from `in`; positions >= n are zero-mass padding at the
+// centre.  Centre: the midpoint of the tile's bounding box, rounded to float
+// (it keeps R, the largest offset, near the box's half-diagonal, which decides
+// how many row blocks may take the tile as far; how close pairs are formed
+// does not depend on the centre).  Header: the centre, the bounding box
+// rounded outward to float, and R = max |x - c| rounded up.  Body records:
+// -D_hi, -D_lo with (D_hi, D_lo) = ds_offset(c, x_hi, x_lo) (pair.cuh).
+// With cid (ensembles), slots whose cid is negative are padding as well.
 template <int TJ>
-__global__ void __launch_bounds__(TJ) rel_tile_kernel(int n, SoA7 in, const int* __restrict__ order,
-                                                      JBodyRel* __restrict__ out,
-                                                      const int* __restrict__ cid) {
-  __shared__ double med[3];
-  const int tid = threadIdx.x;
+__global__ void __launch_bounds__(TJ) rel_tile_nf_kernel(int n, SoA7 in, JBodyNF* __restrict__ out,
+                                                         const int* __restrict__ cid = nullptr) {
+  __shared__ double box[6][TJ / 32];
+  __shared__ float rmax[TJ / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int slot = blockIdx.x * TJ + tid;
-  int b = slot < n ? order[slot] : -1;
-  if (b >= 0 && cid && cid[b] < 0) b = -1;
+  const bool valid = slot < n && (!cid || cid[slot] >= 0);
   double p[3] = {0.0, 0.0, 0.0}, m = 0, vx = 0, vy = 0, vz = 0;
-  if (b >= 0) {
-    p[0] = in.x[b]; p[1] = in.y[b]; p[2] = in.z[b]; m = in.m[b];
-    vx = in.vx[b]; vy = in.vy[b]; vz = in.vz[b];
+  if (valid) {
+    p[0] = in.x[slot]; p[1] = in.y[slot]; p[2] = in.z[slot]; m = in.m[slot];
+    vx = in.vx[slot]; vy = in.vy[slot]; vz = in.vz[slot];
   }
-  if (tid < 3) med[tid] = 0.0;
-  const int nv = __syncthreads_count(b >= 0);
-  if (tid < 32 && nv > 0) {
-    const int ns = min(32, nv);
-    // sample `tid` = slot tid * nv / 32 (all distinct when nv >= 32)
-    const int q = ns == 32 ? static_cast<int>((static_cast<long long>(tid) * nv) >> 5) : tid;
-    const int bq = q < ns || ns == 32 ? order[blockIdx.x * TJ + q] : -1;
-    double s[3] = {0.0, 0.0, 0.0};
-    if (tid < ns) {
-      s[0] = in.x[bq]; s[1] = in.y[bq]; s[2] = in.z[bq];
-    }
+  // bounding box in double (empty tile: +inf/-inf)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {  // rank among the ns samples (ties by lane)
-      int r = 0;
-      for (int l = 0; l < ns; ++l) {
-        const double w = __shfl_sync(0xffffffffu, s[k], l);
-        r += (w < s[k] || (w == s[k] && l < tid)) ? 1 : 0;
-      }
-      if (tid < ns && r == ns / 2) med[k] = s[k];
+  for (int k = 0; k < 6; ++k) {
+    double w = k < 3 ? (valid ? p[k] : INFINITY) : (valid ? p[k - 3] : -INFINITY);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, w, o);
+      w = k < 3 ? fmin(w, u) : fmax(w, u);
     }
+    if (lane == 0) box[k][warp] = w;
   }
   __syncthreads();
-  float c[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) c[k] = isfinite(med[k]) ? static_cast<float>(med[k]) : 0.0f;
-  JBodyRel* tile = out + static_cast<size_t>(blockIdx.x) * (TJ + 1);
-  if (tid == 0) {
-    JBodyRel h;
-    h.x = make_float2(c[0], c[0]); h.y = make_float2(c[1], c[1]); h.z = make_float2(c[2], c[2]);
-    h.m = h.vx = h.vy = h.vz = h.pad = make_float2(0.f, 0.f);
-    tile[0] = h;
-  }
-  float o[3];
+  double lo[3], hi[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    const float hi = static_cast<float>(p[k]);
-    const float lo = static_cast<float>(p[k] - static_cast<double>(hi));
-    o[k] = b >= 0 ? -__fsub_rn(__fsub_rn(c[k], hi), lo) : 0.0f;
+    lo[k] = box[k][0];
+    hi[k] = box[3 + k][0];
+    for (int q = 1; q < TJ / 32; ++q) {
+      lo[k] = fmin(lo[k], box[k][q]);
+      hi[k] = fmax(hi[k], box[3 + k][q]);
+    }
+  }
+  float c[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double mid = 0.5 * lo[k] + 0.5 * hi[k];
+    c[k] = isfinite(mid) ? static_cast<float>(mid) : 0.0f;
+  }
+  // largest offset from the (float) centre, rounded up
+  double r2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double d = p[k] - static_cast<double>(c[k]);
+    r2 += valid ? d * d : 0.0;
+  }
+  float R = __double2float_ru(sqrt(r2));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) R = fmaxf(R, __shfl_xor_sync(0xffffffffu, R, o));
+  if (lane == 0) rmax[warp] = R;
+  __syncthreads();
+  JBodyNF* tile = out + static_cast<size_t>(blockIdx.x) * (TJ + 1);
+  if (tid == 0) {
+    for (int q = 1; q < TJ / 32; ++q) R = fmaxf(R, rmax[q]);
+    JBodyNF h;
+    h.x = make_float2(c[0], c[0]); h.y = make_float2(c[1], c[1]); h.z = make_float2(c[2], c[2]);
+    h.m = make_float2(__double2float_rd(lo[0]), __double2float_rd(lo[1]));
+    h.vx = make_float2(__double2float_rd(lo[2]), __double2float_ru(hi[0]));
+    h.vy = make_float2(__double2float_ru(hi[1]), __double2float_ru(hi[2]));
+    h.vz = make_float2(R, 0.f);
+    h.pad = h.xl = h.yl = h.zl = h.pad2 = make_float2(0.f, 0.f);
+    tile[0] = h;
+  }
+  float oh[3], ol[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float hv = static_cast<float>(p[k]);
+    const float lv = static_cast<float>(p[k] - static_cast<double>(hv));
+    float dh = 0.f, dl = 0.f;
+    if (valid) ds_offset(c[k], hv, lv, dh, dl);
+    oh[k] = -dh;
+    ol[k] = -dl;
   }
   const float fm = static_cast<float>(m), fu = static_cast<float>(vx);
   const float fv = static_cast<float>(vy), fw = static_cast<float>(vz);
-  JBodyRel r;
-  r.x = make_float2(o[0], o[0]); r.y = make_float2(o[1], o[1]); r.z = make_float2(o[2], o[2]);
+  JBodyNF r;
+  r.x = make_float2(oh[0], oh[0]); r.y = make_float2(oh[1], oh[1]); r.z = make_float2(oh[2], oh[2]);
   r.m = make_float2(fm, fm);
   r.vx = make_float2(fu, fu); r.vy = make_float2(fv, fv); r.vz = make_float2(fw, fw);
   r.pad = make_float2(0.f, 0.f);
+  r.xl = make_float2(ol[0], ol[0]); r.yl = make_float2(ol[1], ol[1]); r.zl = make_float2(ol[2], ol[2]);
+  r.pad2 = make_float2(0.f, 0.f);
   tile[1 + tid] = r;
+}
+
+// Gathers rows [0, n) of up to kMaxGather float64 arrays through a position
+// map: dst[a][q] = src[a][ord[q]] (and, with perm_out, perm_out[q] =
+// perm[ord[q]], or ord[q] without perm).  Re-orders an engine's state into
+// Morton order, or a caller's input.
+constexpr int kMaxGather = 13;
+struct GatherArgs {
+  const double* src[kMaxGather];
+  double* dst[kMaxGather];
+  int arrays;
+};
+static __global__ void gather_rows_kernel(int n, const int* __restrict__ ord, GatherArgs g,
+                                          const int* __restrict__ perm, int* __restrict__ perm_out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int src = ord[q];
+#pragma unroll
+  for (int a = 0; a < kMaxGather; ++a)
+    if (a < g.arrays) g.dst[a][q] = g.src[a][src];
+  if (perm_out) perm_out[q] = perm ? perm[src] : src;
+}
+
+// The inverse: dst[a][perm[p]] = src[a][p] for rows [0, n) (back to the
+// caller's body order).
+static __global__ void scatter_rows_kernel(int n, const int* __restrict__ perm, GatherArgs g) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int dst = perm[p];
+#pragma unroll
+  for (int a = 0; a < kMaxGather; ++a)
+    if (a < g.arrays) g.dst[a][dst] = g.src[a][p];
+}
+
+static __global__ void iota_kernel(int n, int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = i;
 }
 
 }  // namespace nbody

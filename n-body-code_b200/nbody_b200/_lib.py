@@ -68,6 +68,9 @@ class NBodyTimers(C.Structure):
         ("step_kernels", C.c_int),
         ("reorders", C.c_longlong),
         ("order_kernels", C.c_int),
+        ("dt_crit", C.c_double),
+        ("tiling_source", C.c_int),
+        ("near_tile_fraction", C.c_double),
     ]
 
 

@@ -34,10 +34,13 @@ class Engine:
     """One system of n bodies on one GPU (wraps nbody_create/nbody_destroy).
 
     precision "mixed" takes pair_variant (nbody_config.pair_variant): 0 picks
-    the tile-relative kernel (4) from 8192 bodies and the packed hi/lo kernel
-    (3) below; 1 and 2 are the other hi/lo forms.  sort_every sets how often
-    the tile-relative kernel re-orders the bodies (0 = every 16 steps).
-    eps2 must be >= 1e-24 in mixed precision."""
+    the near/far tile-relative kernel (4) from 8192 bodies and the packed
+    hi/lo kernel (3) below; 1 and 2 are the other hi/lo forms; 5 is the
+    tile-relative kernel with every tile taken as far (a comparison).  The
+    tile-relative engines keep their bodies in Morton order on the device;
+    get_state and get_derivs return them in the caller's order.  sort_every
+    sets how often they re-order (0 = every 16 steps).  eps2 must be >= 1e-24
+    in mixed precision."""
 
     def __init__(self, n: int, eps2: float = 1e-7, precision: str = "fp64", device: int = 0,
                  dt: float | None = None, eta: float = 1e-2, eta0: float = 1e-4,

@@ -125,3 +125,156 @@ def test_ordering_is_what_keeps_offsets_small():
     e_tiles = vec_rel(model_acc(s, eps2, ordered=True), ref)
     e_plain = vec_rel(model_acc(s, eps2, ordered=False), ref)
     assert np.percentile(e_plain, 99) >= 30 * np.percentile(e_tiles, 99)
+
+
+# ---------------------------------------------------------------------------
+# Near/far tile-relative kernel (pair.cuh RowsMixedNF, reltiles.cuh
+# rel_tile_nf_kernel): bodies in Morton order, warps of consecutive positions,
+# and per (warp rows, tile) either the one-add form on float offsets (far:
+# boxes apart by d > 0 with d >= R/2) or double-single offsets (near).
+# ---------------------------------------------------------------------------
+U = 2.0 ** -24
+
+
+def ds_offset(c, xh, xl):
+    """(hi, lo) = c - (xh + xl) in double-single: TwoSum of c - xh, the low
+    part folded in, renormalised by a second TwoSum; float32 rounding per
+    operation as in the kernel."""
+    c, xh, xl = F32(c), np.asarray(xh, F32), np.asarray(xl, F32)
+    s = c - xh
+    bb = s - c
+    e = (c - (s - bb)) - (xh + bb)
+    t = e - xl
+    hi = s + t
+    b2 = hi - s
+    lo = (s - (hi - b2)) + (t - b2)
+    return hi, lo
+
+
+def test_ds_offset_is_double_single_accurate():
+    rng = np.random.default_rng(3)
+    for scale in (1e-3, 1.0, 40.0):
+        x = rng.normal(0, scale, 5000)
+        h, l = hi_lo(x[None])
+        for c in (F32(0.0), F32(scale * 0.37), F32(-scale * 1.9)):
+            hi, lo = ds_offset(c, h[0], l[0])
+            exact = float(c) - (h[0].astype(np.float64) + l[0].astype(np.float64))
+            got = hi.astype(np.float64) + lo.astype(np.float64)
+            assert np.all(np.abs(got - exact) <= 2.0 ** -44 * np.abs(exact) + 1e-300)
+
+
+def model_acc_near_far(s, eps2, TJ=128, ROWS=128, kappa=0.5):
+    """Accelerations from the near/far kernel's separations (the rest of the
+    pair math in FP64) and the share of (warp rows, tile) pairs taken as near:
+    tiles of TJ and warps of ROWS consecutive Morton positions, tile centre =
+    the midpoint of its bounding box, far iff the boxes are apart by
+    d > 0 with d >= kappa R."""
+    P = np.stack([s["x"], s["y"], s["z"]])
+    n = P.shape[1]
+    order = morton_order(P)
+    Q = P[:, order]                       # engine positions (Morton order)
+    m = s["m"][order]
+    h, l = hi_lo(Q)
+    acc = np.zeros((3, n))
+    near = total = 0
+    for t0 in range(0, n, TJ):
+        j = np.arange(t0, min(n, t0 + TJ))
+        c = (0.5 * Q[:, j].min(1) + 0.5 * Q[:, j].max(1)).astype(F32)
+        R = np.sqrt(((Q[:, j] - c[:, None].astype(np.float64)) ** 2).sum(0)).max()
+        tlo, thi = Q[:, j].min(1), Q[:, j].max(1)
+        Dj = [ds_offset(c[k], h[k, j], l[k, j]) for k in range(3)]
+        for r0 in range(0, n, ROWS):
+            i = np.arange(r0, min(n, r0 + ROWS))
+            blo, bhi = Q[:, i].min(1), Q[:, i].max(1)
+            gap = np.maximum(0, np.maximum(blo - thi, tlo - bhi))
+            d2 = (gap ** 2).sum()
+            far = d2 > 0 and d2 >= (kappa * R) ** 2
+            total += 1
+            near += 0 if far else 1
+            r = np.empty((3, i.size, j.size))
+            for k in range(3):
+                if far:
+                    Di = (F32(c[k]) - h[k, i]) - l[k, i]
+                    r[k] = (Di[:, None] + (-Dj[k][0])[None, :]).astype(np.float64)
+                else:
+                    Dih, Dil = ds_offset(c[k], h[k, i], l[k, i])
+                    r[k] = ((Dih[:, None] + (-Dj[k][0])[None, :]) +
+                            (Dil[:, None] + (-Dj[k][1])[None, :])).astype(np.float64)
+            s2 = (r ** 2).sum(0) + eps2
+            acc[:, i] += (m[j][None, None, :] * r / s2[None] ** 1.5).sum(2)
+    out = np.zeros_like(acc)
+    out[:, order] = acc
+    return out, near / total
+
+
+def model_acc_hilo(s, eps2):
+    """Accelerations from the hi/lo kernel's separations (rest in FP64)."""
+    P = np.stack([s["x"], s["y"], s["z"]])
+    h, l = hi_lo(P)
+    r = np.stack([((h[k][None, :] - h[k][:, None]) + (l[k][None, :] - l[k][:, None])).astype(np.float64)
+                  for k in range(3)])
+    s2 = (r ** 2).sum(0) + eps2
+    return (s["m"][None, None, :] * r / s2[None] ** 1.5).sum(2)
+
+
+def near_fraction(P, TJ=128, ROWS=128, kappa=0.5):
+    """Share of (warp rows, tile) pairs the near/far kernel takes as near, for
+    bodies P (3, n) with n a multiple of TJ and ROWS (vectorised classifier)."""
+    Q = P[:, morton_order(P)]
+    n = Q.shape[1]
+    T = Q.reshape(3, n // TJ, TJ)
+    tlo, thi = T.min(2), T.max(2)
+    c = (0.5 * tlo + 0.5 * thi).astype(F32).astype(np.float64)
+    R = np.sqrt(((T - c[:, :, None]) ** 2).sum(0)).max(1)
+    B = Q.reshape(3, n // ROWS, ROWS)
+    blo, bhi = B.min(2), B.max(2)
+    near = 0
+    for b0 in range(0, blo.shape[1], 64):
+        gap = np.maximum(0, np.maximum(blo[:, b0:b0 + 64, None] - thi[:, None, :],
+                                       tlo[:, None, :] - bhi[:, b0:b0 + 64, None]))
+        d2 = (gap ** 2).sum(0)
+        near += (~((d2 > 0) & (d2 >= (kappa * R[None, :]) ** 2))).sum()
+    return near / (blo.shape[1] * T.shape[1])
+
+
+def test_near_far_separations_keep_the_hilo_accuracy():
+    """Far tiles (one add) and near tiles (double-single) together: per-body
+    accelerations as accurate as the hi/lo kernel's (max and p99 within 1.5x),
+    where plain tile-relative offsets lose more than an order of magnitude on
+    the worst bodies (64-body tiles and warps so that far tiles occur at this
+    size)."""
+    n, eps2 = 8192, 1e-4
+    for s in (nb.plummer(n, seed=5), _two_clusters(n)):
+        ref = O.force(s, eps2)[:3]
+        a, frac = model_acc_near_far(s, eps2, TJ=64, ROWS=64)
+        e_nf = vec_rel(a, ref)
+        e_hl = vec_rel(model_acc_hilo(s, eps2), ref)
+        assert 0.2 < frac < 0.8, frac
+        assert e_nf.max() <= 1.5 * e_hl.max(), (e_nf.max(), e_hl.max())
+        assert np.quantile(e_nf, 0.99) <= 1.5 * np.quantile(e_hl, 0.99)
+
+
+def test_near_share_falls_with_system_size():
+    """The near (three-add) share of the work at the kernel's default shape
+    (128-body tiles, warps of 128 rows): about a quarter at N = 65536."""
+    fr = {n: near_fraction(np.stack([nb.plummer(n, seed=1)[k] for k in ("x", "y", "z")]))
+          for n in (16384, 65536)}
+    assert fr[65536] < 0.3 and fr[65536] < fr[16384], fr
+
+
+def test_far_tiles_bound_the_separation_error():
+    """A far pair's separation from float offsets has error <= 9u |r| (u =
+    2^-24): about u (3 |r| + 3 R) with |x_i - c| <= |r| + R and |r| >= d >= R/2."""
+    rng = np.random.default_rng(4)
+    c = F32(0.75)
+    R = 0.01
+    xj = 0.75 + rng.uniform(-R, R, (3000, 3)) / np.sqrt(3)
+    dirs = rng.normal(size=(3000, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    xi = xj + dirs * rng.uniform(0.5 * R + 2 * R, 50 * R, (3000, 1))   # d >= R/2 from the tile's box
+    hi_, li = hi_lo(xi.T)
+    hj, lj = hi_lo(xj.T)
+    r = np.stack([((c - hi_[k]) - li[k]) + (-((c - hj[k]) - lj[k])) for k in range(3)]).astype(np.float64)
+    exact = (hj.astype(np.float64) + lj) - (hi_.astype(np.float64) + li)
+    err = np.linalg.norm(r - exact, axis=0)
+    assert np.all(err <= 9 * U * np.linalg.norm(exact, axis=0))
