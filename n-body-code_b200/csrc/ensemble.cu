@@ -15,13 +15,15 @@
 // corrector, so results are bitwise reproducible.
 //
 // A step is memset(counter) -> predict -> persistent pair -> correct,
-// captured once into a CUDA graph (mixed, tile-relative: the j-tile records
-// are rebuilt right after predict; every sort_every steps a second captured
-// graph re-orders each cluster's bodies along the Morton curve of its own
-// bounding box first - one global stable sort of (cluster, Morton code) keys,
-// which leaves every cluster in its own padded segment).  Each cluster has its own softening and
-// fixed shared step (the adaptive criterion is per system in the reference,
-// src/nbody.cpp:198-222; ensembles here run fixed steps).
+// captured once into a CUDA graph.  Mixed ensembles use the near/far
+// tile-relative kernel (pair.cuh RowsMixedNF): each cluster keeps its bodies
+// in Morton order within its own padded segment (every sort_every steps a
+// second captured graph sorts (cluster, Morton code) keys over all rows and
+// gathers the state into that order; perm maps positions back to the
+// caller's rows), and the j-tile records are rebuilt right after predict.
+// Each cluster has its own softening and fixed shared step (the adaptive
+// criterion is per system in the reference, src/nbody.cpp:198-222; ensembles
+// here run fixed steps).
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
