@@ -245,7 +245,7 @@ def run_arm(w, precision, state, torch, dist, world, dev, steps, warmup, variant
     step_ms = [s.elapsed_time(t) for s, t in zip(starts, ends)]
     tm = e.timers()  # near_tile_fraction: the last timed step's pair pass
     # kernels of the timed steps: the captured step graph each step, plus the
-    # captured Morton re-ordering where one ran (tile-relative kernel)
+    # captured Hilbert re-ordering where one ran (tile-relative kernel)
     launches = tm["step_kernels"] * steps + tm["order_kernels"] * (tm["reorders"] - reorders0)
     if time_units > 0:  # carry on (untimed) to the requested model time
         rest = int(round(time_units / w.dt)) - warmup - steps

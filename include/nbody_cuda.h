@@ -72,7 +72,7 @@ typedef struct {
                          kernel, FP64 accumulators in registers, 3 = packed
                          hi/lo kernel, FP64 accumulators in shared memory,
                          4 = near/far tile-relative packed-pair kernel: the
-                         engine keeps its bodies in Morton order and cuts
+                         engine keeps its bodies in Hilbert order and cuts
                          them into j-tiles with float offsets from each
                          tile's centre; a tile far from a warp's rows
                          (separated by at least half its radius) costs one
@@ -83,7 +83,7 @@ typedef struct {
                          kernel with every tile taken as far (plain
                          tile-relative offsets; a comparison)               */
   int sort_every;     /* tile-relative kernels: re-order the bodies along
-                         the Morton curve every this many steps (tile
+                         the Hilbert curve every this many steps (tile
                          centres and offsets are rebuilt every step);
                          0 = 16                                             */
 } nbody_config;
@@ -102,9 +102,9 @@ typedef struct {
   int record_format;                /* j-records of the pair kernel in use:
                                        0 FP64, 1 FP32 hi/lo, 2 packed hi/lo,
                                        3 packed near/far tile-relative
-                                       (bodies kept in Morton order)       */
+                                       (bodies kept in Hilbert order)       */
   int step_kernels;                 /* kernel launches in one captured step */
-  long long reorders;               /* Morton re-orderings run by steps     */
+  long long reorders;               /* Hilbert re-orderings run by steps     */
   int order_kernels;                /* kernel launches in one re-ordering   */
   double dt_crit;                   /* criterion of the last completed pass:
                                        after a step, the Aarseth shared step
@@ -193,7 +193,7 @@ const char* nbody_status_string(nbody_status s);
  * host->device and back inside the call (the reference contract).
  * precision = NBODY_MIXED: the near/far tile-relative kernel from 32768
  * bodies over the full row range (each call orders the bodies along the
- * Morton curve in device memory and returns results in the caller's order),
+ * Hilbert curve in device memory and returns results in the caller's order),
  * the packed hi/lo kernel below that and for partial row ranges. */
 nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin, int i_end,
                                      const double* x, const double* y, const double* z,
@@ -262,7 +262,7 @@ typedef struct {
                             kernel shape) chosen by timing when tune = 1    */
   int tune;
   int pair_variant;      /* mixed only: 0 = near/far tile-relative kernel
-                            (each cluster kept in Morton order within its
+                            (each cluster kept in Hilbert order within its
                             segment; default), 3 = packed hi/lo kernel,
                             5 = tile-relative with every tile taken as far
                             (nbody_config numbering)                       */
@@ -276,7 +276,7 @@ typedef struct {
   double last_step_ms;           /* CUDA events around the last graph step */
   int record_format;             /* as nbody_timers.record_format          */
   int step_kernels;              /* kernel launches in one captured step   */
-  long long reorders;            /* Morton re-orderings run by steps       */
+  long long reorders;            /* Hilbert re-orderings run by steps       */
   int order_kernels;             /* kernel launches in one re-ordering     */
 } nbody_ensemble_info_t;
 

@@ -7,9 +7,9 @@
 //   jb64   [ld] JBody64      FP64 j-records (also used by the potential)
 //   jb32   [ld] JBody32      mixed-precision j-records (mixed engines):
 //                            JBody32, JBodyX2, or tiles of JBodyNF
-//   sort   keys, indices, CUB scratch of the Morton ordering (mixed engines)
+//   sort   keys, indices, CUB scratch of the Hilbert ordering (mixed engines)
 //   perm   [2][ld] int       position -> caller's body index (tile-relative
-//                            engines keep their state in Morton order)
+//                            engines keep their state in Hilbert order)
 //   scratch [13][ld]         re-ordered state, gathered caller input, or
 //                            output on its way back to the caller's order
 //   ctl    StepCtl           dt, t, Aarseth criterion, step counter
@@ -19,7 +19,7 @@
 // tile-relative kernel's records come from rel_tile_nf_kernel right after),
 // pair (O(N^2)), correct (O(N), fused split reduction + snap/crackle +
 // correction + dt criterion) - is captured once into a CUDA graph and
-// replayed.  The Morton re-ordering of a tile-relative engine's state is a
+// replayed.  The Hilbert re-ordering of a tile-relative engine's state is a
 // second captured graph, replayed ahead of every sort_every-th step.
 #include <cuda_runtime.h>
 
@@ -54,7 +54,7 @@ constexpr int kPad = 256;        // body padding granularity (multiple of every 
 constexpr int kMaxSplit = 64;    // split-j upper bound
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
 constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
-constexpr int kMortonBits = 48;     // Morton key width (morton_key_kernel)
+constexpr int kOrderBits = 48;     // Hilbert key width (order_key_kernel)
 constexpr int kMaxPotSplit = 32;    // j-splits of the potential diagnostic
 
 thread_local std::string g_last_error;
@@ -129,7 +129,7 @@ const std::vector<PairKernel>& registry() {
       make_fp64<128, 1, 128, 2>(),  make_fp64<128, 4, 128, 1>(),  make_fp64<256, 1, 128, 4>(),
       make_fp64<256, 2, 128, 1>(),  make_fp64<128, 2, 256, 1>(),  make_fp64<64, 2, 128, 1>(),
       make_fp64<128, 2, 128, 1, 6>(), make_fp64<128, 2, 64, 1, 6>(), make_fp64<128, 1, 128, 4, 8>(),
-      // near/far tile-relative packed pairs (bodies in Morton order; default
+      // near/far tile-relative packed pairs (bodies in Hilbert order; default
       // mixed: 128 x 4 rows, j-unroll 2, 4 CTAs/SM = 128 registers, no spills)
       make_mixed_nf<128, 4, 128, 1, 2, 4>(), make_mixed_nf<64, 4, 128>(), make_mixed_nf<128, 2, 128>(),
       make_mixed_nf<256, 2, 128>(), make_mixed_nf<256, 4, 128>(), make_mixed_nf<128, 2, 64>(),
@@ -216,8 +216,8 @@ struct nbody_engine {
   JBody64* jb64 = nullptr;
   void* jb32 = nullptr;  // mixed records: JBody32 or JBodyX2 (sized for the larger)
   JBody64* jbe = nullptr;  // records of the energy diagnostic (never a pair kernel's input)
-  // Morton ordering (mixed engines).  A tile-relative engine keeps its state
-  // in Morton order: position p holds the caller's body perm[p].
+  // Hilbert ordering (mixed engines).  A tile-relative engine keeps its state
+  // in Hilbert order: position p holds the caller's body perm[p].
   uint64_t* sort_keys = nullptr;  // [2][ld]: keys, sorted keys
   int* sort_idx = nullptr;        // [2][ld]: positions, sorted positions (= order)
   double* bbox_part = nullptr;    // [kMaxBBoxParts][6]
@@ -226,7 +226,7 @@ struct nbody_engine {
   int* perm = nullptr;            // [2][ld]: position -> body index, and its re-ordered copy
   double* scratch = nullptr;      // [13][ld]: re-ordered state / gathered caller input / un-permuted output
   unsigned long long* near_count = nullptr;  // near tiles of the last near/far pair launch
-  bool sorted = false;            // the state is in (recent) Morton order
+  bool sorted = false;            // the state is in (recent) Hilbert order
   bool permuted = false;          // perm is not the identity
   int since_sort = 0;             // steps since the last re-ordering
   StepCtl* ctl = nullptr;
@@ -240,7 +240,7 @@ struct nbody_engine {
   // bodies, packed hi/lo below.  Engines re-order every sort_every steps;
   // the drop-in re-orders on every call and raises the threshold.
   int rel_min_bodies = 8192;
-  cudaGraphExec_t order_graph = nullptr;  // captured Morton re-ordering (variant 0)
+  cudaGraphExec_t order_graph = nullptr;  // captured Hilbert re-ordering (variant 0)
   cudaStream_t aux = nullptr;              // drop-in: uploads that overlap the ordering
   cudaEvent_t aux_ev[2] = {nullptr, nullptr};
   int order_kernels = 0;
@@ -269,8 +269,8 @@ int default_format(const nbody_engine* e) {
   return effective_variant(e) >= 4 ? kRecRel : kRecX2;
 }
 
-// The engine keeps its bodies in Morton order (positions != body indices).
-bool morton_resident(const nbody_engine* e);
+// The engine keeps its bodies in Hilbert order (positions != body indices).
+bool curve_resident(const nbody_engine* e);
 
 nbody_status check_status_word(nbody_engine* e) {
   int h = 0;
@@ -407,7 +407,7 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   float best = 1e30f;
   int best_idx = -1, best_split = 1;
   const auto& reg = registry();
-  // the near/far kernel's cost depends on the bodies being in Morton order
+  // the near/far kernel's cost depends on the bodies being in Hilbert order
   if (default_format(e) == kRecRel && e->have_state && !e->sorted)
     NB_TRY(enqueue_reorder_state(e, e->stream));
   for (size_t idx = 0; idx < reg.size(); ++idx) {
@@ -502,20 +502,20 @@ SoA6 own_derivs(nbody_engine* e) {
   return SoA6{D, D + ld, D + 2 * ld, D + 3 * ld, D + 4 * ld, D + 5 * ld};
 }
 
-// Morton order of bodies [0, n) of `in` (bounding box, keys, stable sort):
+// Hilbert order of bodies [0, n) of `in` (bounding box, keys, stable sort):
 // sort_idx + ld then holds, for each sorted position q, the index in `in` of
 // the body that goes there.
-nbody_status enqueue_morton_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
+nbody_status enqueue_curve_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
   const int parts = std::min(kMaxBBoxParts, (n + kBBoxThreads - 1) / kBBoxThreads);
   bbox_partial_kernel<<<parts, kBBoxThreads, 0, st>>>(n, in, e->bbox_part);
   NB_CUDA(cudaGetLastError());
   const size_t ld = e->ld;
-  morton_key_kernel<<<(n + kBBoxThreads - 1) / kBBoxThreads, kBBoxThreads, 0, st>>>(
+  order_key_kernel<<<(n + kBBoxThreads - 1) / kBBoxThreads, kBBoxThreads, 0, st>>>(
       n, in, e->bbox_part, parts, e->sort_keys, e->sort_idx);
   NB_CUDA(cudaGetLastError());
   size_t bytes = e->sort_tmp_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + ld,
-                                          e->sort_idx, e->sort_idx + ld, n, 0, kMortonBits, st));
+                                          e->sort_idx, e->sort_idx + ld, n, 0, kOrderBits, st));
   return NBODY_OK;
 }
 
@@ -529,12 +529,12 @@ GatherArgs gather_args(const double* src, double* dst, size_t ld, int arrays) {
   return g;
 }
 
-// Re-orders the engine's own state into the Morton order of its current
+// Re-orders the engine's own state into the Hilbert order of its current
 // positions: keys and sort, a gather of all 13 state arrays (and of perm)
 // into scratch, and a copy back.  Capturable (the re-ordering graph).
 nbody_status enqueue_reorder_state(nbody_engine* e, cudaStream_t st) {
   const size_t ld = e->ld;
-  NB_TRY(enqueue_morton_order(e, e->n, own_inputs(e), st));
+  NB_TRY(enqueue_curve_order(e, e->n, own_inputs(e), st));
   gather_rows_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
       e->n, e->sort_idx + ld, gather_args(e->state, e->scratch, ld, 13), e->perm, e->perm + ld);
   NB_CUDA(cudaGetLastError());
@@ -548,7 +548,7 @@ nbody_status enqueue_reorder_state(nbody_engine* e, cudaStream_t st) {
 }
 
 // Near/far tile records of bodies [0, n) of `in`, which must already be in
-// Morton order (positions).
+// Hilbert order (positions).
 nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int tj) {
   JBodyNF* out = static_cast<JBodyNF*>(e->jb32);
   const int tiles = e->ld / tj;
@@ -564,7 +564,7 @@ nbody_status build_rel_tiles(nbody_engine* e, int n, const SoA7& in, cudaStream_
 
 // Writes the j-records of a pair kernel's format: FP64 records (hi/lo
 // kernels: also theirs), or tiles of tj near/far records of `in`, which must
-// then be in Morton order.  (The energy diagnostic packs its own records.)
+// then be in Hilbert order.  (The energy diagnostic packs its own records.)
 nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st, int fmt,
                          int tj) {
   if (fmt != kRecRel) {
@@ -579,7 +579,7 @@ nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st
 }
 
 // acc + jerk of n bodies given in any order (`in`, device arrays) with the
-// near/far kernel, after enqueue_morton_order(in): a gather of `in` into
+// near/far kernel, after enqueue_curve_order(in): a gather of `in` into
 // scratch in that order, tiles, the pair pass, and the split reduction
 // written back through the order into `out` (the caller's body order).
 // Leaves the engine's own state alone.
@@ -605,12 +605,12 @@ int tiling_fmt(const nbody_engine* e) { return e->tiled ? e->tiling.k->fmt : kRe
 int tiling_tj(const nbody_engine* e) { return e->tiled ? e->tiling.k->tj : 0; }
 int sort_period(const nbody_engine* e) { return e->cfg.sort_every > 0 ? e->cfg.sort_every : 16; }
 
-bool morton_resident(const nbody_engine* e) { return tiling_fmt(e) == kRecRel; }
+bool curve_resident(const nbody_engine* e) { return tiling_fmt(e) == kRecRel; }
 
 // Before a step of the engine's own state: re-order when the order is stale
 // (never made since set_state, or sort_every steps old).
 nbody_status maybe_reorder(nbody_engine* e, cudaStream_t st) {
-  if (!morton_resident(e)) return NBODY_OK;
+  if (!curve_resident(e)) return NBODY_OK;
   if (!e->sorted || e->since_sort >= sort_period(e)) {
     if (e->order_graph && st == e->stream) {
       NB_CUDA(cudaGraphLaunch(e->order_graph, st));
@@ -629,7 +629,7 @@ nbody_status maybe_reorder(nbody_engine* e, cudaStream_t st) {
 // acc + jerk of the engine's current X, V, M into D (rows [0, n)).
 nbody_status eval_current(nbody_engine* e) {
   NB_TRY(ensure_tiling(e));
-  if (morton_resident(e) && !e->sorted) NB_TRY(enqueue_reorder_state(e, e->stream));
+  if (curve_resident(e) && !e->sorted) NB_TRY(enqueue_reorder_state(e, e->stream));
   NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   if (!e->init_events) {
     NB_CUDA(cudaEventCreate(&e->ev_init[0]));
@@ -719,7 +719,7 @@ nbody_status build_step_graph(nbody_engine* e) {
     return fail(NBODY_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
   }
   if (tiling_fmt(e) == kRecRel && !e->order_graph) {
-    // the Morton re-ordering of the engine's own state, replayed every
+    // the Hilbert re-ordering of the engine's own state, replayed every
     // sort_every steps ahead of the step graph
     const bool sorted = e->sorted, permuted = e->permuted;
     const int since = e->since_sort;
@@ -861,7 +861,7 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
       NB_CUDA(cudaMalloc(&e->bbox_part, sizeof(double) * 6 * kMaxBBoxParts));
       NB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, e->sort_tmp_bytes, e->sort_keys,
                                               e->sort_keys + ld, e->sort_idx, e->sort_idx + ld,
-                                              static_cast<int>(ld), 0, kMortonBits, e->stream));
+                                              static_cast<int>(ld), 0, kOrderBits, e->stream));
       NB_CUDA(cudaMalloc(&e->sort_tmp, std::max<size_t>(e->sort_tmp_bytes, 16)));
     }
     NB_CUDA(cudaMalloc(&e->ctl, sizeof(StepCtl)));
@@ -936,7 +936,7 @@ nbody_status nbody_set_state(nbody_engine* e, const double* x, const double* y, 
     NB_CUDA(cudaGetLastError());
   }
   e->sorted = e->permuted = false;
-  if (!morton_resident(e))
+  if (!curve_resident(e))
     NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, tiling_fmt(e), tiling_tj(e)));
   NB_CUDA(cudaStreamSynchronize(e->stream));
   e->have_state = true;
@@ -1134,8 +1134,8 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   NB_TRY(ensure_partials(e, t.split));
   const SoA7 in{x, y, z, m, vx, vy, vz};
   const SoA6 out{ax, ay, az, jx, jy, jz};
-  if (t.k->fmt == kRecRel) {  // Morton order of the caller's bodies, gathered into scratch
-    NB_TRY(enqueue_morton_order(e, n, in, st));
+  if (t.k->fmt == kRecRel) {  // Hilbert order of the caller's bodies, gathered into scratch
+    NB_TRY(enqueue_curve_order(e, n, in, st));
     return eval_foreign_rel(e, t, n, in, out, st);
   }
   NB_TRY(launch_pack(e, n, in, st, t.k->fmt, t.k->tj));
@@ -1211,11 +1211,11 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   const bool full = i_begin == 0 && i_end == n;
   if (!full) NB_TRY(get_tiling(e, i_end - i_begin, &t));
   // a row range: the packed hi/lo kernel, whose rows stay in the caller's
-  // order (the near/far kernel evaluates all rows in Morton order)
+  // order (the near/far kernel evaluates all rows in Hilbert order)
   if (!full && t.k->fmt == kRecRel) NB_TRY(hilo_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
   if (t.k->fmt == kRecRel) {
-    // positions first: their Morton ordering runs while the masses and
+    // positions first: their Hilbert ordering runs while the masses and
     // velocities upload on a second stream
     if (!e->aux) {
       NB_CUDA(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
@@ -1228,9 +1228,9 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     for (int k = 3; k < 7; ++k)
       NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->aux));
     NB_CUDA(cudaEventRecord(e->aux_ev[1], e->aux));
-    NB_TRY(enqueue_morton_order(e, n, own_inputs(e), e->stream));
+    NB_TRY(enqueue_curve_order(e, n, own_inputs(e), e->stream));
     NB_CUDA(cudaStreamWaitEvent(e->stream, e->aux_ev[1], 0));
-    // the caller's bodies gathered into Morton order, derivatives back in body order
+    // the caller's bodies gathered into Hilbert order, derivatives back in body order
     NB_TRY(eval_foreign_rel(e, t, n, own_inputs(e), own_derivs(e), e->stream));
   } else {
     for (int k = 0; k < 7; ++k)

@@ -17,8 +17,8 @@
 // A step is memset(counter) -> predict -> persistent pair -> correct,
 // captured once into a CUDA graph.  Mixed ensembles use the near/far
 // tile-relative kernel (pair.cuh RowsMixedNF): each cluster keeps its bodies
-// in Morton order within its own padded segment (every sort_every steps a
-// second captured graph sorts (cluster, Morton code) keys over all rows and
+// in Hilbert order within its own padded segment (every sort_every steps a
+// second captured graph sorts (cluster, Hilbert code) keys over all rows and
 // gathers the state into that order; perm maps positions back to the
 // caller's rows), and the j-tile records are rebuilt right after predict.
 // Each cluster has its own softening and fixed shared step (the adaptive
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kBlock) ens_bbox_kernel(const ClusterDev* __re
     if (threadIdx.x == q) bbox[blockIdx.x * 6 + q] = v[q];
 }
 
-// keys[r] = (segment cluster << 48) | 48-bit Morton code (16 bits per axis)
+// keys[r] = (segment cluster << 48) | 48-bit Hilbert index (16 bits per axis)
 // in the cluster's box; padding rows take the segment's largest key, so the
 // sorted rows of cluster c fill exactly its padded segment, bodies first.
 __global__ void ens_key_kernel(int L, const int* __restrict__ cid, const int* __restrict__ seg,
@@ -153,13 +153,15 @@ __global__ void ens_key_kernel(int L, const int* __restrict__ cid, const int* __
     key |= 0xffffffffffffull;
   } else {
     constexpr double kCells = 65535.0;
+    uint32_t cell[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double lo = bbox[c * 6 + k], w = bbox[c * 6 + 3 + k] - lo;
       double q = w > 0.0 ? (X[k * L + r] - lo) * (kCells / w) : 0.0;
       q = fmin(fmax(q, 0.0), kCells);  // NaN -> 0
-      key |= morton_spread21(static_cast<uint32_t>(q)) << k;
+      cell[k] = static_cast<uint32_t>(q);
     }
+    key |= hilbert_key48(cell[0], cell[1], cell[2]);
   }
   keys[r] = key;
   vals[r] = r;
@@ -334,8 +336,8 @@ struct nbody_ensemble {
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool have_derivs = false;
   long long steps = 0;
-  // Morton ordering (mixed, tile-relative variants): each cluster keeps its
-  // bodies in Morton order within its segment; position r holds the body of
+  // Hilbert ordering (mixed, tile-relative variants): each cluster keeps its
+  // bodies in Hilbert order within its segment; position r holds the body of
   // padded row perm[r] (the caller's order).
   int near = 1;                   // near/far kernel (variant 0) or every tile far (5)
   int* perm = nullptr;            // [2][L]
@@ -427,7 +429,7 @@ nbody_status launch_ens_pair(nbody_ensemble* e) {
   return NBODY_OK;
 }
 
-// Morton order of every cluster's bodies within its padded segment.
+// Hilbert order of every cluster's bodies within its padded segment.
 nbody_status ens_order(nbody_ensemble* e, cudaStream_t st) {
   ens_bbox_kernel<<<e->C, kBlock, 0, st>>>(e->cl, e->X, e->L, e->bbox);
   ens_key_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, st>>>(e->L, e->cid, e->seg, e->X,
@@ -440,7 +442,7 @@ nbody_status ens_order(nbody_ensemble* e, cudaStream_t st) {
   return NBODY_OK;
 }
 
-// Puts every cluster's bodies into Morton order within its segment: the
+// Puts every cluster's bodies into Hilbert order within its segment: the
 // order of ens_order, a gather of all 13 state arrays (and of perm) into
 // scratch, and a copy back.  Capturable (the re-ordering graph).
 nbody_status ens_reorder_state(nbody_ensemble* e, cudaStream_t st) {
@@ -463,7 +465,7 @@ nbody_status ens_reorder_state(nbody_ensemble* e, cudaStream_t st) {
 }
 
 // Near/far tile records (tiles of the kernel's TJ) of the state, which is in
-// Morton order within each cluster segment.
+// Hilbert order within each cluster segment.
 nbody_status ens_tiles(nbody_ensemble* e, cudaStream_t st) {
   const size_t L = e->L;
   const SoA7 in{e->X, e->X + L, e->X + 2 * L, e->M, e->V, e->V + L, e->V + 2 * L};
@@ -519,7 +521,7 @@ nbody_status use_kernel(nbody_ensemble* e, const EnsKernel* k) {
 }
 
 nbody_status launch_ens_pack(nbody_ensemble* e) {
-  if (e->fmt == kRecRel && !e->sorted)  // tile-relative: bodies into Morton order first
+  if (e->fmt == kRecRel && !e->sorted)  // tile-relative: bodies into Hilbert order first
     EN_TRY(ens_reorder_state(e, e->stream));
   ens_pack_kernel<<<(e->L + kBlock - 1) / kBlock, kBlock, 0, e->stream>>>(
       e->L, e->cid, e->X, e->V, e->M, e->jb64, e->fmt == kRecX2 ? e->jbx : nullptr);

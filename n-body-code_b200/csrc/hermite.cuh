@@ -241,7 +241,7 @@ static __global__ void correct_kernel(int n, int ld, int S, const double* __rest
 // With a status word (callers that cannot read it back before using the
 // outputs), a non-zero word - a pair kernel gave up a bounded wait - makes
 // every output NaN instead.  With an index map, row i is written to
-// out[c][index[i]] (partials kept in Morton order, outputs in the caller's
+// out[c][index[i]] (partials kept in Hilbert order, outputs in the caller's
 // body order).
 static __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int S,
                                      const double* __restrict__ P, SoA6 out,

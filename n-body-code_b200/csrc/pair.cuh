@@ -30,7 +30,7 @@
 //          of the pair math in float with the MUFU rsqrt, float partial sums
 //          over one j-tile flushed into double accumulators after each tile.
 //   Mixed, near/far tile-relative (default for large systems): bodies in
-//          Morton order, j-tiles of float offsets from each tile's centre;
+//          Hilbert order, j-tiles of float offsets from each tile's centre;
 //          the separation costs one add per component for tiles far from a
 //          warp's rows and is formed in double-single for near tiles
 //          (RowsMixedNF below), so close pairs keep the hi/lo accuracy.
@@ -525,7 +525,7 @@ __device__ __forceinline__ void pair_terms_x2(int p, uint64_t dx, uint64_t dy, u
 }
 
 // Near/far tile-relative rows (the default mixed kernel for large systems).
-// The engine keeps its bodies in Morton order, and each warp takes 32 * IPT
+// The engine keeps its bodies in Hilbert order, and each warp takes 32 * IPT
 // consecutive positions (row k of lane l is warp_row0 + 32 k + l), so a
 // warp's rows occupy a compact region, whose bounding box begin_rows records.
 // Each j-tile is then classified per warp (a warp-uniform branch):
@@ -535,7 +535,7 @@ __device__ __forceinline__ void pair_terms_x2(int p, uint64_t dx, uint64_t dy, u
 //          is at most about 2^-24 (3 |r| + 3 R) <= 9 * 2^-24 |r|, float
 //          accuracy of the separation itself.
 //   near - everything else (the warp's own tiles, its neighbours, and tiles
-//          whose box straddles a jump of the Morton curve): the separation in
+//          whose boxes are wide for their body count): the separation in
 //          double-single, r = (D_hi(x_i) - D_hi(x_j)) + (D_lo(x_i) - D_lo(x_j))
 //          with (D_hi, D_lo) = ds_offset(c, x_hi, x_lo), three adds per
 //          component like the hi/lo kernel, so close pairs keep float
@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(NT, MINB) pair_mixed_x2_kernel(const JBodyX2* 
 }
 
 // Near/far tile-relative mixed kernel: tile t is TJ + 1 records at
-// jt + t*(TJ + 1) (header first); i-rows (engine positions, Morton order) come
+// jt + t*(TJ + 1) (header first); i-rows (engine positions, Hilbert order) come
 // from a.rows, clamped below a.n_rows_pad; rows >= a.i_end are not stored and
 // stay out of the warps' bounding boxes.
 template <int NT, int IPT, int TJ, int ACC_SMEM = 1, int JU = 1, int MINB = 1, int NEAR = 1>
@@ -865,7 +865,7 @@ __device__ __forceinline__ void pair_ensemble(const typename R::JB* __restrict__
 // Near/far tile-relative ensemble: tiles of TJ + 1 records over the whole
 // padded array (cluster segments are multiples of 256 rows, so a tile never
 // spans two clusters); i-rows from the FP64 state `rows`, whose bodies each
-// cluster keeps in Morton order within its segment.  R is a RowsMixedNF.
+// cluster keeps in Hilbert order within its segment.  R is a RowsMixedNF.
 template <class R>
 __global__ void __launch_bounds__(R::NT) ensemble_pair_nf_kernel(
     const JBodyNF* __restrict__ jt, const EnsItem* __restrict__ items, int n_items,

@@ -1,13 +1,13 @@
-// Morton ordering and the j-records of the near/far tile-relative mixed
+// Hilbert ordering and the j-records of the near/far tile-relative mixed
 // kernel (JBodyNF, pair.cuh).
 //
-// Bodies are ordered along a Morton (Z-order) curve of their positions; the
+// Bodies are ordered along a Hilbert curve of their positions; the
 // engine keeps its state in that order (re-ordered every sort_every steps),
 // so each j-tile of TJ consecutive positions covers a compact region and
 // stores its bodies as offsets from the tile's centre.
 //
 //   bbox_partial_kernel   per-CTA min/max of x, y, z          (O(N) read, 24 B/body)
-//   morton_key_kernel     48-bit key (16 bits per axis) + index (O(N), 24 B in, 12 B out)
+//   order_key_kernel      48-bit Hilbert key (16 bits per axis) + index (O(N), 24 B in, 12 B out)
 //   (stable radix sort of (key, index) pairs: cub::DeviceRadixSort)
 //   gather_rows_kernel    the state (13 arrays) or a caller's input into that order
 //   scatter_rows_kernel   back to the caller's order (downloads, outputs)
@@ -27,7 +27,7 @@ namespace nbody {
 constexpr int kBBoxThreads = 256;
 
 // Interleaves the low 21 bits of v with two zero bits between each.
-__device__ __forceinline__ uint64_t morton_spread21(uint32_t v) {
+__device__ __forceinline__ uint64_t spread21(uint32_t v) {
   uint64_t x = v & 0x1fffffull;
   x = (x | (x << 32)) & 0x1f00000000ffffull;
   x = (x | (x << 16)) & 0x1f0000ff0000ffull;
@@ -35,6 +35,37 @@ __device__ __forceinline__ uint64_t morton_spread21(uint32_t v) {
   x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
   x = (x | (x << 2)) & 0x1249249249249249ull;
   return x;
+}
+
+// 48-bit Hilbert index of a point given its 16-bit cell coordinates, by
+// Skilling's transpose algorithm (J. Skilling, "Programming the Hilbert
+// curve", AIP Conf. Proc. 707, 2004): the axes are turned into the curve's
+// transposed index by inverting and exchanging low bits level by level, Gray
+// decoding follows, and the three 16-bit words are interleaved, axis 0 most
+// significant.  Consecutive indices are neighbouring cells (no jumps, unlike
+// a Morton curve), so runs of consecutive bodies cover compact regions.
+__device__ __forceinline__ uint64_t hilbert_key48(uint32_t a0, uint32_t a1, uint32_t a2) {
+  uint32_t X[3] = {a0, a1, a2};
+  for (uint32_t Q = 1u << 15; Q > 1u; Q >>= 1) {
+    const uint32_t P = Q - 1u;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t Q = 1u << 15; Q > 1u; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1u;
+  return (spread21(X[0] ^ t) << 2) | (spread21(X[1] ^ t) << 1) |
+         spread21(X[2] ^ t);
 }
 
 __device__ __forceinline__ double warp_min(double v) {
@@ -83,9 +114,10 @@ static __global__ void __launch_bounds__(kBBoxThreads) bbox_partial_kernel(int n
     if (threadIdx.x == k) part[blockIdx.x * 6 + k] = v[k];
 }
 
-// keys[i] = Morton code of body i in the box of the nparts partial boxes;
-// vals[i] = i.  Non-finite coordinates map to cell 0.
-static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
+// keys[i] = Hilbert index of body i's cell (2^16 cells per axis) in the box
+// of the nparts partial boxes; vals[i] = i.  Non-finite coordinates map to
+// cell 0.
+static __global__ void __launch_bounds__(kBBoxThreads) order_key_kernel(
     int n, SoA7 in, const double* __restrict__ part, int nparts, uint64_t* __restrict__ keys,
     int* __restrict__ vals) {
   __shared__ double sh[6 * 32];
@@ -99,20 +131,20 @@ static __global__ void __launch_bounds__(kBBoxThreads) morton_key_kernel(
   if (i >= n) return;
   constexpr double kCells = 65535.0;  // 2^16 - 1 cells per axis: a 48-bit key
   const double p[3] = {in.x[i], in.y[i], in.z[i]};
-  uint64_t key = 0;
+  uint32_t cell[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const double w = v[k + 3] - v[k];
     double q = w > 0.0 ? (p[k] - v[k]) * (kCells / w) : 0.0;
     q = fmin(fmax(q, 0.0), kCells);  // NaN -> 0
-    key |= morton_spread21(static_cast<uint32_t>(q)) << k;
+    cell[k] = static_cast<uint32_t>(q);
   }
-  keys[i] = key;
+  keys[i] = hilbert_key48(cell[0], cell[1], cell[2]);
   vals[i] = i;
 }
 
 
-// Records of the near/far kernel from bodies already in Morton order: tile t
+// Records of the near/far kernel from bodies already in Hilbert order: tile t
 // (CTA t, TJ threads) = header + the bodies at positions t*TJ + k, k < TJ, read
 // straight (coalesced) from `in`; positions >= n are zero-mass padding at the
 // centre.  Centre: the midpoint of the tile's bounding box, rounded to float
@@ -212,7 +244,7 @@ __global__ void __launch_bounds__(TJ) rel_tile_nf_kernel(int n, SoA7 in, JBodyNF
 // Gathers rows [0, n) of up to kMaxGather float64 arrays through a position
 // map: dst[a][q] = src[a][ord[q]] (and, with perm_out, perm_out[q] =
 // perm[ord[q]], or ord[q] without perm).  Re-orders an engine's state into
-// Morton order, or a caller's input.
+// Hilbert order, or a caller's input.
 constexpr int kMaxGather = 13;
 struct GatherArgs {
   const double* src[kMaxGather];

@@ -37,7 +37,7 @@ class Engine:
     the near/far tile-relative kernel (4) from 8192 bodies and the packed
     hi/lo kernel (3) below; 1 and 2 are the other hi/lo forms; 5 is the
     tile-relative kernel with every tile taken as far (a comparison).  The
-    tile-relative engines keep their bodies in Morton order on the device;
+    tile-relative engines keep their bodies in Hilbert order on the device;
     get_state and get_derivs return them in the caller's order.  sort_every
     sets how often they re-order (0 = every 16 steps).  eps2 must be >= 1e-24
     in mixed precision."""

@@ -51,7 +51,7 @@ class Ensemble:
     """Clusters of sizes n[c] with softening eps2[c] and fixed step dt[c].
 
     Mixed precision: pair_variant 0 (default) uses the near/far tile-relative
-    kernel, each cluster kept in Morton order within its own segment (states
+    kernel, each cluster kept in Hilbert order within its own segment (states
     and derivatives come back in the caller's order); 3 uses the packed hi/lo
     kernel; 5 the tile-relative kernel with every tile taken as far."""
 

@@ -126,7 +126,7 @@ def test_dropin_row_range_mixed(n):
     """Mixed drop-in: a row range gives the full call's rows.  At 3000 bodies
     both calls run the packed hi/lo kernel (only the split of the j-sum may
     differ); at 40000 the full call runs the near/far kernel on the bodies in
-    Morton order and the row range the hi/lo kernel, so the two agree to the
+    Hilbert order and the row range the hi/lo kernel, so the two agree to the
     mixed kernels' accuracy, and both match the FP64 direct sums."""
     s = nb.plummer(n, seed=4)
     full = nb.force_calculation(s, eps2=1e-4, precision="mixed")
@@ -358,7 +358,7 @@ def test_max_size_sampled_rows(precision):
 
 # ---------------------------------------------------------------------------
 # Tile-relative mixed kernel (pair_variant 4; the automatic choice from 8192
-# bodies): j-bodies in Morton-ordered tiles, positions as float offsets from
+# bodies): j-bodies in Hilbert-ordered tiles, positions as float offsets from
 # the tile centre.
 # ---------------------------------------------------------------------------
 REL = dict(pair_variant=4)
@@ -424,7 +424,7 @@ def test_tile_relative_deterministic_and_order_free():
 
 def test_tile_relative_device_entry_and_steps():
     """Caller-owned device arrays (n below the engine's size), then Hermite
-    runs against the FP64 engine with the Morton order refreshed every step
+    runs against the FP64 engine with the Hilbert order refreshed every step
     and every 16 steps."""
     import torch
     n, eps2 = 3000, 1e-4
@@ -564,7 +564,7 @@ def test_near_tiles_keep_close_pairs_accurate(n):
 
 
 def test_near_far_kernel_reports_its_near_share_and_keeps_caller_order():
-    """The near/far engine keeps its bodies in Morton order: its energy equals
+    """The near/far engine keeps its bodies in Hilbert order: its energy equals
     the FP64 engine's on the same bodies (order-independent sums), its state
     comes back in the caller's order, and a Plummer sphere of 65536 bodies
     sends a minority of (warp, tile) pairs down the double-single path."""

@@ -1,20 +1,21 @@
 """CPU model of the tile-relative separations of the mixed pair kernel.
 
-The kernel (pair.cuh RowsMixedRel, reltiles.cuh rel_tile_kernel) orders the
-j-bodies along a Morton curve, cuts them into tiles, and stores each body as
--D(x) with D(x) = fl(fl(c - x_hi) - x_lo) for the tile centre c (a float);
-an i-row forms D(x_i) with the same float operations and r_ij = D(x_i) +
-(-D(x_j)).  This file restates that arithmetic in numpy float32 (one
-rounding per operation, like the kernel's sub.rn / add.rn) and checks the
-properties the design relies on:
+The one-add tile-relative form (the far tiles of pair.cuh RowsMixedNF, and
+every tile with pair_variant 5) stores each body of a tile as -D(x) with
+D(x) = fl(fl(c - x_hi) - x_lo) for the tile centre c (a float); an i-row forms
+D(x_i) with the same float operations and r_ij = D(x_i) + (-D(x_j)).  This file
+restates that arithmetic in numpy float32 (one rounding per operation, like
+the kernel's sub.rn / add.rn) and checks the properties the design relies on:
 
 * the self pair cancels exactly, whatever the tile centre;
-* the separation error stays at about one float ulp of |x - c| per side,
-  so with Morton tiles the accelerations keep the mixed accuracy class
-  against the FP64 oracle;
-* without the Morton order (tiles of arbitrary bodies) the same arithmetic
-  loses accuracy wherever close pairs sit far from the tiles' centres (a
-  tight cluster beside a wide one) - the ordering keeps the offsets local.
+* the separation error stays at about one float ulp of |x - c| per side, so
+  with tiles of spatially ordered bodies the accelerations stay in the mixed
+  accuracy class, and without an order (tiles of arbitrary bodies) close
+  pairs far from their tiles' centres lose accuracy;
+* the near/far kernel (bodies in Hilbert order, double-single separations on
+  near tiles, reltiles.cuh rel_tile_nf_kernel) keeps the hi/lo kernel's
+  accuracy, bounds the far tiles' separation error, and sends a small share
+  of the work down the double-single path.
 """
 import numpy as np
 
@@ -129,11 +130,55 @@ def test_ordering_is_what_keeps_offsets_small():
 
 # ---------------------------------------------------------------------------
 # Near/far tile-relative kernel (pair.cuh RowsMixedNF, reltiles.cuh
-# rel_tile_nf_kernel): bodies in Morton order, warps of consecutive positions,
+# rel_tile_nf_kernel): bodies in Hilbert order, warps of consecutive positions,
 # and per (warp rows, tile) either the one-add form on float offsets (far:
 # boxes apart by d > 0 with d >= R/2) or double-single offsets (near).
 # ---------------------------------------------------------------------------
 U = 2.0 ** -24
+
+
+def hilbert_keys(q):
+    """48-bit Hilbert indices of 16-bit cells q (3, n): Skilling's transpose
+    algorithm, as the engine's hilbert_key48 (reltiles.cuh) computes them."""
+    X = [q[k].astype(np.uint64).copy() for k in range(3)]
+    Q = np.uint64(1 << 15)
+    while Q > 1:
+        Pm = Q - np.uint64(1)
+        for i in range(3):
+            m = (X[i] & Q) != 0
+            X[0] = np.where(m, X[0] ^ Pm, X[0])
+            t = np.where(m, np.uint64(0), (X[0] ^ X[i]) & Pm)
+            X[0] ^= t
+            X[i] ^= t
+        Q >>= np.uint64(1)
+    X[1] ^= X[0]
+    X[2] ^= X[1]
+    t = np.zeros_like(X[0])
+    Q = np.uint64(1 << 15)
+    while Q > 1:
+        t = np.where((X[2] & Q) != 0, t ^ (Q - np.uint64(1)), t)
+        Q >>= np.uint64(1)
+    return (_spread16(X[0] ^ t) << np.uint64(2)) | (_spread16(X[1] ^ t) << np.uint64(1)) | _spread16(X[2] ^ t)
+
+
+def hilbert_order(P):
+    """Stable order of the Hilbert indices of bodies P (3, n) over their
+    bounding box (2^16 cells per axis), as order_key_kernel sorts them."""
+    lo, hi = P.min(1), P.max(1)
+    q = np.clip((P - lo[:, None]) * (65535.0 / (hi - lo))[:, None], 0, 65535).astype(np.uint64)
+    return np.argsort(hilbert_keys(q), kind="stable")
+
+
+def test_hilbert_keys_trace_a_continuous_curve():
+    """Consecutive Hilbert indices are face-neighbouring cells: the 8^3 cells
+    of the top three levels (multiples of 2^13), sorted by key, step by
+    exactly one cell every time, and the keys are distinct."""
+    g = np.stack(np.meshgrid(*[np.arange(8)] * 3, indexing="ij")).reshape(3, -1)
+    keys = hilbert_keys((g * 8192).astype(np.uint64))
+    assert np.unique(keys).size == keys.size
+    o = np.argsort(keys)
+    steps = np.abs(np.diff(g[:, o], axis=1)).sum(0)
+    assert np.all(steps == 1)
 
 
 def ds_offset(c, xh, xl):
@@ -171,7 +216,7 @@ def model_acc_near_far(s, eps2, TJ=128, ROWS=128, kappa=0.5):
     d > 0 with d >= kappa R."""
     P = np.stack([s["x"], s["y"], s["z"]])
     n = P.shape[1]
-    order = morton_order(P)
+    order = hilbert_order(P)
     Q = P[:, order]                       # engine positions (Morton order)
     m = s["m"][order]
     h, l = hi_lo(Q)
@@ -220,7 +265,7 @@ def model_acc_hilo(s, eps2):
 def near_fraction(P, TJ=128, ROWS=128, kappa=0.5):
     """Share of (warp rows, tile) pairs the near/far kernel takes as near, for
     bodies P (3, n) with n a multiple of TJ and ROWS (vectorised classifier)."""
-    Q = P[:, morton_order(P)]
+    Q = P[:, hilbert_order(P)]
     n = Q.shape[1]
     T = Q.reshape(3, n // TJ, TJ)
     tlo, thi = T.min(2), T.max(2)
@@ -256,10 +301,11 @@ def test_near_far_separations_keep_the_hilo_accuracy():
 
 def test_near_share_falls_with_system_size():
     """The near (three-add) share of the work at the kernel's default shape
-    (128-body tiles, warps of 128 rows): about a quarter at N = 65536."""
+    (128-body tiles, warps of 128 rows): about an eighth at N = 65536 with
+    Hilbert order (Morton order, whose jumps make wide tiles: a quarter)."""
     fr = {n: near_fraction(np.stack([nb.plummer(n, seed=1)[k] for k in ("x", "y", "z")]))
           for n in (16384, 65536)}
-    assert fr[65536] < 0.3 and fr[65536] < fr[16384], fr
+    assert fr[65536] < 0.2 and fr[65536] < fr[16384], fr
 
 
 def test_far_tiles_bound_the_separation_error():
