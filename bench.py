@@ -583,7 +583,7 @@ def run_ensemble(a, torch, world, rank, dist, dev, steps, warmup, time_units):
              for k in nb.FIELDS}
     dt = 1.0 / 512
     inter = float((sizes_all.astype(np.float64) ** 2).sum())
-    variant = a.variant if a.precision == "mixed" and a.variant in (3, 5) else 0
+    variant = a.variant if a.precision == "mixed" and a.variant in (3, 4, 5) else 0
     ens = nb.Ensemble(sizes, eps2, dt, precision=a.precision, tune=True, pair_variant=variant)
     ens.set_state(state)
     ens.force_calculation()

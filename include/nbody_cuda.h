@@ -261,12 +261,15 @@ typedef struct {
   int tiles_per_item;    /* j-tiles per work item; 0 = default 8, or (with the
                             kernel shape) chosen by timing when tune = 1    */
   int tune;
-  int pair_variant;      /* mixed only: 0 = near/far tile-relative kernel
-                            (each cluster kept in Hilbert order within its
-                            segment; default), 3 = packed hi/lo kernel,
+  int pair_variant;      /* mixed only: 0 = automatic (the packed hi/lo
+                            kernel, the faster one for clusters of up to a
+                            few thousand bodies), 3 = packed hi/lo kernel,
+                            4 = near/far tile-relative kernel (each cluster
+                            kept in Hilbert order within its segment),
                             5 = tile-relative with every tile taken as far
                             (nbody_config numbering)                       */
-  int sort_every;        /* variant 0: re-order every this many steps; 0 = 16 */
+  int sort_every;        /* variants 4, 5: re-order every this many steps;
+                            0 = 16                                          */
 } nbody_ensemble_config;
 typedef struct {
   int nclusters, padded_rows, items, tiles_per_item, grid;

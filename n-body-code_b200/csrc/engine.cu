@@ -118,7 +118,7 @@ PairKernel make_mixed_nf() {
   return {NBODY_MIXED, NT, IPT, TJ, kRecRel,
           reinterpret_cast<const void*>(&pair_mixed_nf_kernel<NT, IPT, TJ, ACC, JU, MINB, NEAR>),
           2 * (TJ + 1) * sizeof(JBodyNF) + (ACC ? sizeof(double) * 6 * IPT * NT : 0), ACC, JU,
-          MINB, NEAR};
+          MINB, NEAR ? 1 : 0};
 }
 
 // The first entry of each shape/variant is the one explicit tilings select;
@@ -138,6 +138,7 @@ const std::vector<PairKernel>& registry() {
       make_mixed_nf<64, 4, 128, 1, 1, 8>(),  make_mixed_nf<128, 6, 128, 1, 1>(),
       make_mixed_nf<64, 6, 128, 1, 1>(),     make_mixed_nf<128, 4, 128, 1, 2>(),
       make_mixed_nf<128, 4, 64, 1, 2, 4>(),  make_mixed_nf<128, 2, 64, 1, 2, 4>(),
+      make_mixed_nf<128, 4, 128, 1, 2, 4, 2>(), make_mixed_nf<64, 4, 128, 1, 2, 8, 2>(),
       // the same kernel with every tile taken as far (plain tile-relative
       // separations; pair_variant 5, a measured comparison)
       make_mixed_nf<128, 4, 128, 1, 2, 4, 0>(), make_mixed_nf<128, 2, 128, 1, 1, 1, 0>(),

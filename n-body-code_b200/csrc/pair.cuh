@@ -542,7 +542,8 @@ __device__ __forceinline__ void pair_terms_x2(int p, uint64_t dx, uint64_t dy, u
 //          relative accuracy however close they are, and the self pair
 //          cancels exactly.
 // NEAR = 0 takes the far form for every tile (the plain tile-relative
-// kernel, kept as a measured comparison).
+// kernel, kept as a measured comparison); NEAR >= 1 is the near/far kernel
+// with its near loop unrolled NEAR times.
 template <int NT_, int IPT, int TJ_, int ACC_SMEM, int JU, int NEAR>
 struct RowsMixedNF : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
   using Base = RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU>;
@@ -678,7 +679,7 @@ struct RowsMixedNF : RowsMixedX2<NT_, IPT, TJ_, ACC_SMEM, JU> {
 #pragma unroll
     for (int p = 0; p < NP; ++p) fax[p] = fay[p] = faz[p] = fjx[p] = fjy[p] = fjz[p] = 0ull;
     const uint64_t eps2 = this->eps2, m3 = this->m3;
-#pragma unroll 1
+#pragma unroll(NEAR > 1 ? NEAR : 1)
     for (int j = 1; j <= TJ; ++j) {
       const ulonglong2* r = reinterpret_cast<const ulonglong2*>(tile + j);
       const ulonglong2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4], r5 = r[5];

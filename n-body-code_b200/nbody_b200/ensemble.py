@@ -50,10 +50,10 @@ def _f(name):
 class Ensemble:
     """Clusters of sizes n[c] with softening eps2[c] and fixed step dt[c].
 
-    Mixed precision: pair_variant 0 (default) uses the near/far tile-relative
-    kernel, each cluster kept in Hilbert order within its own segment (states
-    and derivatives come back in the caller's order); 3 uses the packed hi/lo
-    kernel; 5 the tile-relative kernel with every tile taken as far."""
+    Mixed precision: pair_variant 0 (default) and 3 use the packed hi/lo
+    kernel; 4 the near/far tile-relative kernel, each cluster kept in Hilbert
+    order within its own segment (states and derivatives come back in the
+    caller's order); 5 the tile-relative kernel with every tile taken as far."""
 
     def __init__(self, n, eps2, dt, precision: str = "mixed", device: int = 0,
                  tiles_per_item: int = 0, tune: bool = False, pair_variant: int = 0,

@@ -86,14 +86,16 @@ def test_ensemble_hermite_steps_vs_single_engines(small_ensemble):
         assert abs(U[c] - Uref) <= 1e-11 * max(abs(Uref), 1e-300) + 1e-300
 
 
-def test_ensemble_deterministic(small_ensemble):
+@pytest.mark.parametrize("variant", [0, 4])
+def test_ensemble_deterministic(small_ensemble, variant):
     sizes, eps2, state = small_ensemble
     outs = []
     for _ in range(2):
-        with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed") as e:
+        with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed", pair_variant=variant) as e:
             e.set_state(state)
             e.timestepping(4)
             outs.append(e.get_state())
+            assert e.info()["record_format"] == (3 if variant == 4 else 2)
     for k in outs[0]:
         assert np.array_equal(outs[0][k], outs[1][k]), k
 
@@ -121,13 +123,13 @@ def test_plummer_ensemble_config():
 
 @pytest.mark.parametrize("tpi", [1, 4, 64])
 def test_ensemble_tile_relative_vs_oracle(small_ensemble, tpi):
-    """Near/far tile-relative ensemble (the mixed default): per cluster against
+    """Near/far tile-relative ensemble (pair_variant 4): per cluster against
     the FP64 oracle within the mixed bounds, and within 3x of the hi/lo
     ensemble's median and worst error (near tiles form separations in
     double-single)."""
     sizes, eps2, state = small_ensemble
     d = {}
-    for name, kw in (("rel", {}), ("hilo", dict(pair_variant=3))):
+    for name, kw in (("rel", dict(pair_variant=4)), ("hilo", {})):
         with nb.Ensemble(sizes, eps2, 1 / 512, precision="mixed", tiles_per_item=tpi, **kw) as e:
             e.set_state(state)
             e.force_calculation()
@@ -155,8 +157,8 @@ def test_ensemble_tile_relative_steps_vs_fp64(small_ensemble):
     cluster stays within mixed-precision distance of the FP64 ensemble."""
     sizes, eps2, state = small_ensemble
     runs = {}
-    for name, prec, kw in (("fp64", "fp64", {}), ("rel1", "mixed", dict(sort_every=1)),
-                           ("rel", "mixed", {})):
+    for name, prec, kw in (("fp64", "fp64", {}), ("rel1", "mixed", dict(sort_every=1, pair_variant=4)),
+                           ("rel", "mixed", dict(pair_variant=4))):
         with nb.Ensemble(sizes, eps2, 1 / 512, precision=prec, **kw) as e:
             e.set_state(state)
             e.timestepping(16)
