@@ -428,8 +428,8 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
       float ms = 0.f;
       NB_CUDA(cudaEventElapsedTime(&ms, a, b));
       if (getenv("NBODY_TUNE_VERBOSE"))
-        fprintf(stderr, "[nbody tune] prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d minb=%d split=%d  %.4f ms\n",
-                k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, k.minb, s, ms / 3);
+        fprintf(stderr, "[nbody tune] #%zu prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d minb=%d split=%d  %.4f ms\n",
+                idx, k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, k.minb, s, ms / 3);
       if (ms < best) {
         best = ms;
         best_idx = static_cast<int>(idx);
