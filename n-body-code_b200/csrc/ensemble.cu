@@ -275,12 +275,12 @@ EnsKernel ens_kernel(int precision) {
           reinterpret_cast<const void*>(&ensemble_pair_kernel<R>), pair_smem_bytes<R>()};
 }
 
-template <class R>
+template <class R, int MINB = 1>
 EnsKernel ens_kernel_nf() {
   static_assert(R::ROWS == kPadRows, "an item's row block is one padding unit");
   return {NBODY_MIXED, R::NT, R::TJ, kRecRel,
-          reinterpret_cast<const void*>(&ensemble_pair_nf_kernel<R>),
-          2 * (R::TJ + 1) * sizeof(JBodyNF) + R::kExtraSmem, R::kNear};
+          reinterpret_cast<const void*>(&ensemble_pair_nf_kernel<R, MINB>),
+          2 * (R::TJ + 1) * sizeof(JBodyNF) + R::kExtraSmem, R::kNear ? 1 : 0};
 }
 
 // The first entry of each (precision, record format, near) is its default.
@@ -295,11 +295,21 @@ const std::vector<EnsKernel>& ens_registry() {
       ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 2, 1>>(),
       ens_kernel_nf<RowsMixedNF<128, 2, 128, 1, 2, 1>>(),
       ens_kernel_nf<RowsMixedNF<64, 4, 128, 1, 2, 1>>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 2>>(),
+      // 64 threads capped at 128 registers: 8 CTAs (16 warps) per SM
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 1>, 8>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 2, 1>, 8>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 2>, 8>(),
+      ens_kernel_nf<RowsMixedNF<64, 4, 128, 1, 1, 1>, 8>(),
       ens_kernel_nf<RowsMixedNF<64, 4, 64, 1, 1, 0>>(),
       ens_kernel_nf<RowsMixedNF<128, 2, 128, 1, 1, 0>>(),
       ens_kernel<RowsMixedX2<64, 4, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<128, 2, 128, 1, 1>>(NBODY_MIXED),
       ens_kernel<RowsMixedX2<64, 4, 64, 1, 1>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<64, 4, 64, 1, 2>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<128, 2, 64, 1, 1>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<128, 2, 64, 1, 2>>(NBODY_MIXED),
+      ens_kernel<RowsMixedX2<64, 4, 64, 0, 2>>(NBODY_MIXED),
   };
   return r;
 }

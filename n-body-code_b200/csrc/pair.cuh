@@ -867,8 +867,8 @@ __device__ __forceinline__ void pair_ensemble(const typename R::JB* __restrict__
 // padded array (cluster segments are multiples of 256 rows, so a tile never
 // spans two clusters); i-rows from the FP64 state `rows`, whose bodies each
 // cluster keeps in Hilbert order within its segment.  R is a RowsMixedNF.
-template <class R>
-__global__ void __launch_bounds__(R::NT) ensemble_pair_nf_kernel(
+template <class R, int MINB = 1>
+__global__ void __launch_bounds__(R::NT, MINB) ensemble_pair_nf_kernel(
     const JBodyNF* __restrict__ jt, const EnsItem* __restrict__ items, int n_items,
     unsigned int* counter, double* P, int* status, RowSrc rows) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
