@@ -117,9 +117,9 @@ def parse():
                     help="tile the pair kernels by the heuristic instead of the autotuner")
     ap.add_argument("--variant", type=int, default=0,
                     help="mixed pair kernel (nbody_config.pair_variant): 0 = automatic (near/far "
-                         "tile-relative from 8192 bodies), 1 = scalar hi/lo, 2/3 = packed hi/lo, "
-                         "4 = near/far tile-relative, 5 = plain tile-relative; ensembles: 3 = packed "
-                         "hi/lo, 5 = plain tile-relative, else near/far")
+                         "tile-relative from 16384 bodies), 1 = scalar hi/lo, 2/3 = packed hi/lo, "
+                         "4 = near/far tile-relative, 5 = plain tile-relative; ensembles: 4 = "
+                         "near/far, 5 = plain tile-relative, else packed hi/lo")
     ap.add_argument("--time-units", type=float, default=1.0,
                     help="integrate to this model time in total (timed steps included, untimed "
                          "beyond them) and report |dE/E| there")

@@ -65,7 +65,7 @@ typedef struct {
   double eta0;        /* initial-dt criterion, default 1e-4 (nbody.h:15)    */
   int tune;           /* 1: time candidate tilings on first use (autotuner) */
   int threads, i_per_thread, j_tile, split_j; /* 0 = choose automatically   */
-  int pair_variant;   /* mixed only: 0 = automatic (variant 4 from 8192
+  int pair_variant;   /* mixed only: 0 = automatic (variant 4 from 16384
                          bodies, variant 3 below, where building the tiles
                          costs more than it saves), 1 = scalar FP32 kernel
                          on hi/lo positions, 2 = packed-pair (f32x2) hi/lo

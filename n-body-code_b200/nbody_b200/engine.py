@@ -34,7 +34,7 @@ class Engine:
     """One system of n bodies on one GPU (wraps nbody_create/nbody_destroy).
 
     precision "mixed" takes pair_variant (nbody_config.pair_variant): 0 picks
-    the near/far tile-relative kernel (4) from 8192 bodies and the packed
+    the near/far tile-relative kernel (4) from 16384 bodies and the packed
     hi/lo kernel (3) below; 1 and 2 are the other hi/lo forms; 5 is the
     tile-relative kernel with every tile taken as far (a comparison).  The
     tile-relative engines keep their bodies in Hilbert order on the device;

@@ -86,7 +86,7 @@ def test_fp64_every_tiling_agrees(tiling):
     dict(threads=128, i_per_thread=4, j_tile=128, split_j=2, pair_variant=1),
     dict(threads=128, i_per_thread=4, j_tile=256, split_j=1, pair_variant=1),
     dict(threads=128, i_per_thread=4, j_tile=128, split_j=9, pair_variant=2),
-    # tile-relative (4; the automatic choice from 8192 bodies)
+    # tile-relative (4; the automatic choice from 16384 bodies)
     dict(threads=128, i_per_thread=4, j_tile=128, split_j=1, pair_variant=4),
     dict(threads=128, i_per_thread=2, j_tile=128, split_j=7, pair_variant=4),
     dict(threads=64, i_per_thread=4, j_tile=128, split_j=64, pair_variant=4),
@@ -357,7 +357,7 @@ def test_max_size_sampled_rows(precision):
 
 
 # ---------------------------------------------------------------------------
-# Tile-relative mixed kernel (pair_variant 4; the automatic choice from 8192
+# Tile-relative mixed kernel (pair_variant 4; the automatic choice from 16384
 # bodies): j-bodies in Hilbert-ordered tiles, positions as float offsets from
 # the tile centre.
 # ---------------------------------------------------------------------------
