@@ -139,11 +139,6 @@ const std::vector<PairKernel>& registry() {
       make_mixed_nf<64, 6, 128, 1, 1>(),     make_mixed_nf<128, 4, 128, 1, 2>(),
       make_mixed_nf<128, 4, 64, 1, 2, 4>(),  make_mixed_nf<128, 2, 64, 1, 2, 4>(),
       make_mixed_nf<128, 4, 128, 1, 2, 4, 2>(), make_mixed_nf<64, 4, 128, 1, 2, 8, 2>(),
-      // 2 rows per thread capped at 64 / 80 registers: 32 / 24 warps per SM
-      make_mixed_nf<128, 2, 128, 1, 2, 8, 1>(), make_mixed_nf<128, 2, 128, 1, 2, 8, 2>(),
-      make_mixed_nf<128, 2, 64, 1, 2, 8, 1>(),  make_mixed_nf<128, 2, 128, 1, 1, 8, 1>(),
-      make_mixed_nf<128, 2, 128, 1, 2, 6, 2>(), make_mixed_nf<128, 2, 128, 1, 2, 6, 1>(),
-      make_mixed_nf<128, 2, 64, 1, 2, 6, 1>(),
       // the same kernel with every tile taken as far (plain tile-relative
       // separations; pair_variant 5, a measured comparison)
       make_mixed_nf<128, 4, 128, 1, 2, 4, 0>(), make_mixed_nf<128, 2, 128, 1, 1, 1, 0>(),
@@ -153,8 +148,6 @@ const std::vector<PairKernel>& registry() {
       make_mixed_x2<128, 2, 128, 1, 1>(),
       make_mixed_x2<128, 4, 64, 1, 1, 5>(), make_mixed_x2<128, 4, 64, 1, 1, 6>(),
       make_mixed_x2<128, 4, 64, 1, 1>(),    make_mixed_x2<64, 4, 64, 1, 1, 10>(),
-      // 2 rows per thread, 32 warps per SM (the ensemble's fastest shape)
-      make_mixed_x2<128, 2, 64, 1, 2, 8>(), make_mixed_x2<128, 2, 128, 1, 2, 8>(),
       // packed pairs, FP64 accumulators in registers
       make_mixed_x2<128, 4, 128, 0, 2>(), make_mixed_x2<128, 2, 128, 0, 2>(),
       make_mixed_x2<256, 2, 128, 0, 2>(), make_mixed_x2<64, 4, 128, 0, 2>(),
