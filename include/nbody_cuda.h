@@ -194,12 +194,24 @@ const char* nbody_status_string(nbody_status s);
  * precision = NBODY_MIXED: the near/far tile-relative kernel from 32768
  * bodies over the full row range (each call orders the bodies along the
  * Hilbert curve in device memory and returns results in the caller's order),
- * the packed hi/lo kernel below that and for partial row ranges. */
+ * the packed hi/lo kernel below that and for partial row ranges.  The
+ * tiling is the heuristic one unless the autotuner has chosen one for the same
+ * device, precision and n in this process (nbody_force_calculation_tune, or an
+ * engine created with tune = 1); the call itself never runs the autotuner. */
 nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin, int i_end,
                                      const double* x, const double* y, const double* z,
                                      const double* m, const double* vx, const double* vy,
                                      const double* vz, double* ax, double* ay, double* az,
                                      double* jx, double* jy, double* jz);
+/* Optional, once per system size: runs the autotuner for full-row
+ * nbody_force_calculation calls of these n bodies (the same arguments as the
+ * call's inputs) on the calling thread's cached engine and keeps its choice
+ * for the process.  Takes about a second at n = 65536 (tens of trial
+ * launches); later calls of this size and precision use the tuned tiling.
+ * No reference counterpart: the reference's back end has no tiling. */
+nbody_status nbody_force_calculation_tune(int n, double eps2, int precision, const double* x,
+                                          const double* y, const double* z, const double* m,
+                                          const double* vx, const double* vy, const double* vz);
 /* Release the cached drop-in engines of the calling thread. */
 nbody_status nbody_force_calculation_release(void);
 

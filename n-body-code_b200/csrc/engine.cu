@@ -243,6 +243,9 @@ struct nbody_engine {
   // sort_every steps; the drop-in re-orders on every call and raises the
   // threshold.
   int rel_min_bodies = 16384;
+  // drop-in engines: reuse a tiling the autotuner chose for the same
+  // (device, precision, record format, size) in this process; never tune
+  bool tune_lookup = false;
   cudaGraphExec_t order_graph = nullptr;  // captured Hilbert re-ordering (variant 0)
   cudaStream_t aux = nullptr;              // drop-in: uploads that overlap the ordering
   cudaEvent_t aux_ev[2] = {nullptr, nullptr};
@@ -392,18 +395,22 @@ nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st
                          int tj);
 nbody_status enqueue_reorder_state(nbody_engine* e, cudaStream_t st);
 
+// The tiling the autotuner cached for this engine's (device, precision,
+// record format, ld, rows), if any.
+bool tuned_lookup(const nbody_engine* e, int rows, Tiling* out) {
+  const auto key = std::make_tuple(e->dev, e->cfg.precision, default_format(e), e->ld, rows);
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tuned.find(key);
+  if (it == g_tuned.end()) return false;
+  out->k = &registry()[it->second.first];
+  out->split = it->second.second;
+  out->source = 3;
+  return true;
+}
+
 nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
   const auto key = std::make_tuple(e->dev, e->cfg.precision, default_format(e), e->ld, rows);
-  {
-    std::lock_guard<std::mutex> g(g_tune_mu);
-    auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) {
-      out->k = &registry()[it->second.first];
-      out->split = it->second.second;
-      out->source = 3;
-      return NBODY_OK;
-    }
-  }
+  if (tuned_lookup(e, rows, out)) return NBODY_OK;
   cudaEvent_t a, b;
   NB_CUDA(cudaEventCreate(&a));
   NB_CUDA(cudaEventCreate(&b));
@@ -470,8 +477,9 @@ nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
     return fail(NBODY_ERR_INVALID_ARG,
                 "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d variant=%d", nt,
                 ipt, tj, variant);
-  if (c.tune && !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j && !c.pair_variant)
-    return autotune(e, rows, out);
+  const bool automatic = !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j && !c.pair_variant;
+  if (c.tune && automatic) return autotune(e, rows, out);
+  if (e->tune_lookup && automatic && tuned_lookup(e, rows, out)) return NBODY_OK;
   out->k = k;
   out->split = c.split_j ? std::min(c.split_j, kMaxSplit) : choose_split(e, *k, rows);
   out->source = 1;
@@ -1172,19 +1180,11 @@ thread_local DropInCache g_dropin;
 
 }  // namespace
 
-extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin,
-                                                int i_end, const double* x, const double* y,
-                                                const double* z, const double* m,
-                                                const double* vx, const double* vy,
-                                                const double* vz, double* ax, double* ay,
-                                                double* az, double* jx, double* jy, double* jz) {
-  TraceRange trace_("nbody_force_calculation");
-  if (n < 1) return fail(NBODY_ERR_INVALID_ARG, "n = %d", n);
-  if (i_begin < 0 || i_end > n || i_begin > i_end)
-    return fail(NBODY_ERR_INVALID_ARG, "row range [%d, %d) outside [0, %d)", i_begin, i_end, n);
-  const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
-  for (auto p : ptrs)
-    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null array");
+namespace {
+
+// The calling thread's cached drop-in engine for (device, precision), made
+// (again) for n bodies and eps2 when those change.
+nbody_status dropin_engine(int n, double eps2, int precision, nbody_engine** out) {
   int dev = 0;
   NB_CUDA(cudaGetDevice(&dev));
   DropIn& d = g_dropin.m[{dev, precision}];
@@ -1202,10 +1202,56 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     // every call re-orders: tile-relative pays off only above ~24k bodies
     // (measured per call: N = 16384 428 vs 357 us hi/lo; N = 65536 it wins)
     d.e->rel_min_bodies = 32768;
+    d.e->tune_lookup = true;
     d.n = n;
     d.eps2 = eps2;
   }
-  nbody_engine* e = d.e;
+  *out = d.e;
+  return NBODY_OK;
+}
+
+}  // namespace
+
+extern "C" nbody_status nbody_force_calculation_tune(int n, double eps2, int precision,
+                                                     const double* x, const double* y,
+                                                     const double* z, const double* m,
+                                                     const double* vx, const double* vy,
+                                                     const double* vz) {
+  TraceRange trace_("nbody_force_calculation_tune");
+  if (n < 1) return fail(NBODY_ERR_INVALID_ARG, "n = %d", n);
+  const void* ptrs[7] = {x, y, z, m, vx, vy, vz};
+  for (auto p : ptrs)
+    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null array");
+  nbody_engine* e = nullptr;
+  NB_TRY(dropin_engine(n, eps2, precision, &e));
+  NB_TRY(nbody_set_state(e, x, y, z, m, vx, vy, vz));  // the bodies the trials run on
+  // the autotuner times the full-row call's kernel family on these bodies
+  // (in curve order for the near/far kernel) and caches its choice for the
+  // process; drop-in calls of this size then look it up
+  e->cfg.tune = 1;
+  e->tiled = false;
+  const nbody_status st = ensure_tiling(e);
+  e->cfg.tune = 0;
+  NB_TRY(st);
+  NB_CUDA(cudaStreamSynchronize(e->stream));
+  return check_status_word(e);
+}
+
+extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precision, int i_begin,
+                                                int i_end, const double* x, const double* y,
+                                                const double* z, const double* m,
+                                                const double* vx, const double* vy,
+                                                const double* vz, double* ax, double* ay,
+                                                double* az, double* jx, double* jy, double* jz) {
+  TraceRange trace_("nbody_force_calculation");
+  if (n < 1) return fail(NBODY_ERR_INVALID_ARG, "n = %d", n);
+  if (i_begin < 0 || i_end > n || i_begin > i_end)
+    return fail(NBODY_ERR_INVALID_ARG, "row range [%d, %d) outside [0, %d)", i_begin, i_end, n);
+  const void* ptrs[13] = {x, y, z, m, vx, vy, vz, ax, ay, az, jx, jy, jz};
+  for (auto p : ptrs)
+    if (!p) return fail(NBODY_ERR_INVALID_ARG, "null array");
+  nbody_engine* e = nullptr;
+  NB_TRY(dropin_engine(n, eps2, precision, &e));
   const size_t ld = e->ld, b = sizeof(double) * n;
   const double* src[7] = {x, y, z, vx, vy, vz, m};
   double* dst[7] = {e->X, e->X + ld, e->X + 2 * ld, e->V, e->V + ld, e->V + 2 * ld, e->M};

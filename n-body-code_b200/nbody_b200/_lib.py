@@ -109,6 +109,7 @@ _SIGS = {
     "nbody_status_string": [C.c_int],
     "nbody_force_calculation": [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int] + [_vp] * 13,
     "nbody_force_calculation_release": [],
+    "nbody_force_calculation_tune": [C.c_int, C.c_double, C.c_int] + [_vp] * 7,
     "nbody_acc_jerk_device": [_eng, C.c_int] + [_vp] * 13 + [_vp],
     "nbody_plummer": [C.c_int, C.c_uint64] + [_vp] * 7,
     "nbody_reference_ic": [C.c_int, C.c_double] + [_vp] * 7,

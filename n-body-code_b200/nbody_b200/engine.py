@@ -194,6 +194,16 @@ def force_calculation(state: dict, eps2: float = 1e-7, precision: str = "fp64", 
     return out
 
 
+def force_calculation_tune(state: dict, eps2: float = 1e-7, precision: str = "fp64") -> None:
+    """Autotune the drop-in's tiling for full-row calls on these bodies
+    (nbody_force_calculation_tune); later force_calculation calls of this size
+    and precision on this thread's device use it."""
+    L = _lib.load()
+    arrs = [_arr(state[k]) for k in FIELDS]
+    check(L.nbody_force_calculation_tune(arrs[0].size, float(eps2), PRECISIONS[precision],
+                                         *map(_ptr, arrs)), "nbody_force_calculation_tune")
+
+
 def release_force_cache() -> None:
     check(_lib.load().nbody_force_calculation_release(), "nbody_force_calculation_release")
 

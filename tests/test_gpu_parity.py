@@ -141,6 +141,33 @@ def test_dropin_row_range_mixed(n):
     assert vec_rel(part[:3, sub], O.force_rows(s, 1e-4, sub)[:3]).max() <= 2e-6
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dropin_tune_keeps_results(precision):
+    """nbody_force_calculation_tune: after the drop-in's autotuner has run for
+    this size, full-row calls (tuned tiling) and row ranges keep the accuracy
+    of the heuristic tiling against the oracle's direct sums."""
+    n = 40000 if precision == "mixed" else 5000
+    eps2 = 1e-4
+    tol, tol_j = (TOL_FP64, TOL_FP64) if precision == "fp64" else (2e-6, 5e-5)
+    s = nb.plummer(n, seed=6)
+    rows = np.arange(0, n, max(1, n // 300))
+    ref = O.force_rows(s, eps2, rows)
+    nb.release_force_cache()
+    try:
+        before = nb.force_calculation(s, eps2=eps2, precision=precision)
+        nb.force_calculation_tune(s, eps2=eps2, precision=precision)
+        after = nb.force_calculation(s, eps2=eps2, precision=precision)
+        part = nb.force_calculation(s, eps2=eps2, precision=precision, i_begin=100, i_end=900)
+    finally:
+        nb.release_force_cache()
+    for d in (before, after):
+        ea, ej = derivs_rel(d[:, rows], ref)
+        assert ea <= tol and ej <= tol_j, (precision, ea, ej)
+    assert np.all(part[:, :100] == 0) and np.all(part[:, 900:] == 0)
+    ea, _ = derivs_rel(part[:, 100:900], after[:, 100:900])
+    assert ea <= tol, ea
+
+
 def test_fp64_deterministic():
     s = nb.plummer(5000, seed=9)
     a = engine_derivs(s, 1e-4)
