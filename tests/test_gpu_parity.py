@@ -392,20 +392,36 @@ REL = dict(pair_variant=4)
 HILO = dict(pair_variant=3)
 
 
-@pytest.mark.parametrize("case", ["plummer", "far_from_origin", "two_clusters"])
+@pytest.mark.parametrize("case", ["plummer", "far_from_origin", "two_clusters", "offset_1e6",
+                                  "flat_disk", "coincident_pairs", "lattice"])
 def test_tile_relative_accuracy_vs_hilo(case):
     """Tile-relative separations stay in the hi/lo kernel's accuracy class:
     per-body acc error against the FP64 oracle within 3x of the hi/lo
-    kernel's (median) and within the mixed bounds, wherever the system sits."""
+    kernel's (median) and within the mixed bounds, wherever the system sits
+    and whatever its shape: a degenerate bounding box (a flat disk), tied
+    Hilbert keys (coincident bodies, a regular lattice) and a system 1e6 units
+    from the origin, where the float hi parts have an ulp of 1/16."""
     n, eps2 = 4096, 1e-4
     s = nb.plummer(n, seed=2)
     if case == "far_from_origin":      # float hi parts alone would lose ~10 bits here
         for k in ("x", "y", "z"):
             s[k] = s[k] + 1000.0
+    elif case == "offset_1e6":
+        for k in ("x", "y", "z"):
+            s[k] = s[k] + 1.0e6
     elif case == "two_clusters":       # a tight cluster 50 units from a wide one
         t = nb.plummer(n, seed=3)
         for k in ("x", "y", "z", "vx", "vy", "vz"):
             s[k] = np.where(np.arange(n) % 2 == 0, s[k], 0.05 * t[k] + (50.0 if k == "x" else 0.0))
+    elif case == "flat_disk":          # every z and vz zero: a box of zero height
+        s["z"], s["vz"] = np.zeros(n), np.zeros(n)
+    elif case == "coincident_pairs":   # body 2k+1 sits on body 2k (softened r = 0 pairs)
+        for k in ("x", "y", "z"):
+            s[k] = np.repeat(s[k][::2], 2)
+    elif case == "lattice":            # 16^3 grid: many equal coordinates
+        g = (np.arange(16) + 0.5) / 16.0
+        X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+        s["x"], s["y"], s["z"] = X.ravel(), Y.ravel(), Z.ravel()
     ref = O.force(s, eps2)
     rel = engine_derivs(s, eps2, precision="mixed", **REL)
     hilo = engine_derivs(s, eps2, precision="mixed", **HILO)
@@ -417,6 +433,43 @@ def test_tile_relative_accuracy_vs_hilo(case):
     assert np.median(er) <= 2e-6 and er.max() <= 2e-4
     assert np.median(er) <= 3 * np.median(eh) + 1e-8
     assert np.median(jr) <= 3 * np.median(jh) + 1e-7
+
+
+def _acc_term_scale(s, eps2, block=256):
+    """sum_j m_j |r_ij| / s_ij^1.5 per body (FP64): the size of the terms an
+    acceleration sums, the scale its rounding errors are relative to."""
+    P = np.stack([s["x"], s["y"], s["z"]])
+    out = np.empty(P.shape[1])
+    for i0 in range(0, P.shape[1], block):
+        d = P[:, None, :] - P[:, i0:i0 + block, None]
+        r2 = (d ** 2).sum(0)
+        out[i0:i0 + block] = (s["m"][None, :] * np.sqrt(r2) / (r2 + eps2) ** 1.5).sum(1)
+    return out
+
+
+def test_tile_relative_on_a_line():
+    """Bodies on one axis: the pulls from both sides cancel, so |a| is far
+    below the terms it sums and every float kernel's error relative to |a|
+    grows on the bodies where they cancel (measured worst 3e-4 for hi/lo, 3e-3
+    for near/far).  Relative to the size of the terms, the near/far error
+    stays within 12x the hi/lo kernel's, as the far tiles' separation bound
+    (9 ulp of |r| against about 1) allows, and below 1e-6 (measured median /
+    max 4.3e-8 / 5.7e-7, hi/lo 1.1e-8 / 2.9e-7)."""
+    n, eps2 = 4096, 1e-4
+    s = nb.plummer(n, seed=2)
+    for k in ("y", "z", "vy", "vz"):
+        s[k] = np.zeros(n)
+    ref = O.force(s, eps2)
+    scale = _acc_term_scale(s, eps2)
+    err = {}
+    for name, kw in (("rel", REL), ("hilo", HILO)):
+        d = engine_derivs(s, eps2, precision="mixed", **kw)
+        err[name] = np.sqrt(((d[:3] - ref[:3]) ** 2).sum(0)) / scale
+    print(f"line: acc error / term scale median rel {np.median(err['rel']):.3e} hilo "
+          f"{np.median(err['hilo']):.3e}; max rel {err['rel'].max():.3e} hilo {err['hilo'].max():.3e}")
+    assert err["rel"].max() <= 1e-6
+    assert err["rel"].max() <= 12 * err["hilo"].max() + 1e-9
+    assert np.median(err["rel"]) <= 12 * np.median(err["hilo"]) + 1e-10
 
 
 @pytest.mark.parametrize("n", (1, 2, 33, 255, 257, 1000))
