@@ -12,7 +12,8 @@
 //   gather_rows_kernel    the state (13 arrays) or a caller's input into that order
 //   scatter_rows_kernel   back to the caller's order (downloads, outputs)
 //   rel_tile_nf_kernel<TJ> tile box, centre and radius; hi/lo offsets per body
-//                         (O(N), 56 B read coalesced, 96 B written per body)
+//                         (O(N), 56 B read coalesced, 96 B written per body,
+//                         one bulk copy per tile from shared memory)
 //
 // Every step is deterministic: the bounding box reduces in a fixed order and
 // the sort is stable, so the records (and the pair sums) are reproducible.
@@ -154,11 +155,13 @@ static __global__ void __launch_bounds__(kBBoxThreads) order_key_kernel(
 // rounded outward to float, and R = max |x - c| rounded up.  Body records:
 // -D_hi, -D_lo with (D_hi, D_lo) = ds_offset(c, x_hi, x_lo) (pair.cuh).
 // With cid (ensembles), slots whose cid is negative are padding as well.
+static_assert(sizeof(JBodyNF) == 96, "tile records are 96 bytes: a tile starts 16-byte aligned");
 template <int TJ>
 __global__ void __launch_bounds__(TJ) rel_tile_nf_kernel(int n, SoA7 in, JBodyNF* __restrict__ out,
                                                          const int* __restrict__ cid = nullptr) {
   __shared__ double box[6][TJ / 32];
   __shared__ float rmax[TJ / 32];
+  __shared__ __align__(128) JBodyNF stage[TJ + 1];  // the tile, written out in one bulk copy
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int slot = blockIdx.x * TJ + tid;
   const bool valid = slot < n && (!cid || cid[slot] >= 0);
@@ -217,7 +220,7 @@ __global__ void __launch_bounds__(TJ) rel_tile_nf_kernel(int n, SoA7 in, JBodyNF
     h.vy = make_float2(__double2float_ru(hi[1]), __double2float_ru(hi[2]));
     h.vz = make_float2(R, 0.f);
     h.pad = h.xl = h.yl = h.zl = h.pad2 = make_float2(0.f, 0.f);
-    tile[0] = h;
+    stage[0] = h;
   }
   float oh[3], ol[3];
 #pragma unroll
@@ -238,7 +241,11 @@ __global__ void __launch_bounds__(TJ) rel_tile_nf_kernel(int n, SoA7 in, JBodyNF
   r.pad = make_float2(0.f, 0.f);
   r.xl = make_float2(ol[0], ol[0]); r.yl = make_float2(ol[1], ol[1]); r.zl = make_float2(ol[2], ol[2]);
   r.pad2 = make_float2(0.f, 0.f);
-  tile[1 + tid] = r;
+  stage[1 + tid] = r;
+  // (TJ + 1) * 96 bytes from a 96-byte multiple: both 16-byte aligned
+  bulk_store_fence();
+  __syncthreads();
+  if (tid == 0) bulk_store(tile, stage, static_cast<uint32_t>(sizeof(JBodyNF) * (TJ + 1)));
 }
 
 // Gathers rows [0, n) of up to kMaxGather float64 arrays through a position

@@ -3,7 +3,9 @@
 // j-body tiles move global -> shared with the non-tensor bulk copy
 // (cp.async.bulk ... mbarrier::complete_tx::bytes), issued by one thread and
 // tracked by an mbarrier transaction count.  Every copy lands in the issuing
-// CTA's own shared memory and reads this GPU's own global memory.
+// CTA's own shared memory and reads this GPU's own global memory.  Tile
+// records go the other way (shared -> global, bulk_group completion) from the
+// record builder.
 // Every wait is bounded by the global nanosecond timer: a wait that runs past
 // its limit reports failure instead of spinning forever.
 #pragma once
@@ -53,6 +55,22 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
           "r"(smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+}
+
+// Own shared memory -> global (bytes % 16 == 0, both addresses 16-byte
+// aligned), issued by one thread after the block's shared-memory writes are
+// made visible to the async proxy (bulk_store_fence + __syncthreads).
+// Returns once the copy has completed: its shared-memory source may then be
+// reused and its global writes are done.
+__device__ __forceinline__ void bulk_store_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_addr(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
