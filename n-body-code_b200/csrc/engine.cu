@@ -55,6 +55,11 @@ constexpr int kMaxSplit = 64;    // split-j upper bound
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
 constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
 constexpr int kOrderBits = 48;     // Hilbert key width (order_key_kernel)
+// The drop-in orders by the top 30 bits (1024 cells per axis, the curve's
+// level-10 cells): four radix passes instead of six on every call.  Bodies
+// that share a cell keep their input order, which moves no tile boundary
+// beyond the cell.
+constexpr int kDropInOrderLowBit = 18;
 constexpr int kMaxPotSplit = 32;    // j-splits of the potential diagnostic
 
 thread_local std::string g_last_error;
@@ -516,7 +521,8 @@ SoA6 own_derivs(nbody_engine* e) {
 // Hilbert order of bodies [0, n) of `in` (bounding box, keys, stable sort):
 // sort_idx + ld then holds, for each sorted position q, the index in `in` of
 // the body that goes there.
-nbody_status enqueue_curve_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st) {
+nbody_status enqueue_curve_order(nbody_engine* e, int n, const SoA7& in, cudaStream_t st,
+                                 int low_bit = 0) {
   const int parts = std::min(kMaxBBoxParts, (n + kBBoxThreads - 1) / kBBoxThreads);
   bbox_partial_kernel<<<parts, kBBoxThreads, 0, st>>>(n, in, e->bbox_part);
   NB_CUDA(cudaGetLastError());
@@ -526,7 +532,8 @@ nbody_status enqueue_curve_order(nbody_engine* e, int n, const SoA7& in, cudaStr
   NB_CUDA(cudaGetLastError());
   size_t bytes = e->sort_tmp_bytes;
   NB_CUDA(cub::DeviceRadixSort::SortPairs(e->sort_tmp, bytes, e->sort_keys, e->sort_keys + ld,
-                                          e->sort_idx, e->sort_idx + ld, n, 0, kOrderBits, st));
+                                          e->sort_idx, e->sort_idx + ld, n, low_bit, kOrderBits,
+                                          st));
   return NBODY_OK;
 }
 
@@ -595,7 +602,7 @@ nbody_status launch_pack(nbody_engine* e, int n, const SoA7& in, cudaStream_t st
 // written back through the order into `out` (the caller's body order).
 // Leaves the engine's own state alone.
 nbody_status eval_foreign_rel(nbody_engine* e, const Tiling& t, int n, const SoA7& in,
-                              const SoA6& out, cudaStream_t st) {
+                              const SoA6& out, cudaStream_t st, bool reduce = true) {
   const size_t ld = e->ld;
   const int* ord = e->sort_idx + ld;
   const double* srcs[7] = {in.x, in.y, in.z, in.m, in.vx, in.vy, in.vz};
@@ -606,6 +613,7 @@ nbody_status eval_foreign_rel(nbody_engine* e, const Tiling& t, int n, const SoA
   const SoA7 sorted{g.dst[0], g.dst[1], g.dst[2], g.dst[3], g.dst[4], g.dst[5], g.dst[6]};
   NB_TRY(build_rel_tiles(e, n, sorted, st, t.k->tj));
   NB_TRY(launch_pair(e, t, 0, n, st, &sorted, n));
+  if (!reduce) return NBODY_OK;  // the caller sums the splits (rows in sort_idx + ld order)
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
       0, n, e->ld, t.split, e->P, out, nullptr, ord);
   NB_CUDA(cudaGetLastError());
@@ -1146,7 +1154,7 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   const SoA7 in{x, y, z, m, vx, vy, vz};
   const SoA6 out{ax, ay, az, jx, jy, jz};
   if (t.k->fmt == kRecRel) {  // Hilbert order of the caller's bodies, gathered into scratch
-    NB_TRY(enqueue_curve_order(e, n, in, st));
+    NB_TRY(enqueue_curve_order(e, n, in, st, kDropInOrderLowBit));
     return eval_foreign_rel(e, t, n, in, out, st);
   }
   NB_TRY(launch_pack(e, n, in, st, t.k->fmt, t.k->tj));
@@ -1263,13 +1271,14 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
   // order (the near/far kernel evaluates all rows in Hilbert order)
   if (!full && t.k->fmt == kRecRel) NB_TRY(hilo_tiling(e, i_end - i_begin, &t));
   NB_TRY(ensure_partials(e, t.split));
+  if (!e->aux) {
+    NB_CUDA(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
+    for (auto& ev : e->aux_ev) NB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  const int* index = nullptr;  // row -> output position (the near/far rows are in Hilbert order)
   if (t.k->fmt == kRecRel) {
     // positions first: their Hilbert ordering runs while the masses and
     // velocities upload on a second stream
-    if (!e->aux) {
-      NB_CUDA(cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
-      for (auto& ev : e->aux_ev) NB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    }
     NB_CUDA(cudaEventRecord(e->aux_ev[0], e->stream));
     NB_CUDA(cudaStreamWaitEvent(e->aux, e->aux_ev[0], 0));
     for (int k = 0; k < 3; ++k)
@@ -1277,29 +1286,37 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     for (int k = 3; k < 7; ++k)
       NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->aux));
     NB_CUDA(cudaEventRecord(e->aux_ev[1], e->aux));
-    NB_TRY(enqueue_curve_order(e, n, own_inputs(e), e->stream));
+    NB_TRY(enqueue_curve_order(e, n, own_inputs(e), e->stream, kDropInOrderLowBit));
     NB_CUDA(cudaStreamWaitEvent(e->stream, e->aux_ev[1], 0));
-    // the caller's bodies gathered into Hilbert order, derivatives back in body order
-    NB_TRY(eval_foreign_rel(e, t, n, own_inputs(e), own_derivs(e), e->stream));
+    // the caller's bodies gathered into Hilbert order; the split sums below
+    // write the derivatives back in body order
+    NB_TRY(eval_foreign_rel(e, t, n, own_inputs(e), own_derivs(e), e->stream, false));
+    index = e->sort_idx + ld;
   } else {
     for (int k = 0; k < 7; ++k)
       NB_CUDA(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, e->stream));
     NB_TRY(launch_pack(e, n, own_inputs(e), e->stream, t.k->fmt, t.k->tj));
     NB_TRY(launch_pair(e, t, i_begin, i_end, e->stream));
-    if (i_end > i_begin) {
-      reduce_splits_kernel<<<(i_end - i_begin + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
-          i_begin, i_end, e->ld, t.split, e->P, own_derivs(e));
-      NB_CUDA(cudaGetLastError());
-    }
   }
+  // one field at a time: field k's download (second stream) overlaps the
+  // split sums of field k + 1
   double* out[6] = {ax, ay, az, jx, jy, jz};
   const size_t rb = sizeof(double) * (i_end - i_begin);
+  const int rows = i_end - i_begin;
   for (int k = 0; k < 6; ++k) {
     if (i_begin > 0) memset(out[k], 0, sizeof(double) * i_begin);
     if (i_end < n) memset(out[k] + i_end, 0, sizeof(double) * (n - i_end));
-    if (rb) NB_CUDA(cudaMemcpyAsync(out[k] + i_begin, e->D + k * ld + i_begin, rb,
-                                    cudaMemcpyDeviceToHost, e->stream));
+    if (!rows) continue;
+    reduce_split_field_kernel<<<(rows + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
+        i_begin, i_end, e->ld, t.split, e->P + k * ld, e->D + k * ld, index);
+    NB_CUDA(cudaGetLastError());
+    NB_CUDA(cudaEventRecord(e->aux_ev[0], e->stream));
+    NB_CUDA(cudaStreamWaitEvent(e->aux, e->aux_ev[0], 0));
+    NB_CUDA(cudaMemcpyAsync(out[k] + i_begin, e->D + k * ld + i_begin, rb, cudaMemcpyDeviceToHost,
+                            e->aux));
   }
+  NB_CUDA(cudaEventRecord(e->aux_ev[1], e->aux));
+  NB_CUDA(cudaStreamWaitEvent(e->stream, e->aux_ev[1], 0));
   return check_status_word(e);  // its read-back follows the outputs; one wait for all
 }
 

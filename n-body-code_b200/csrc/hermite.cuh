@@ -262,6 +262,23 @@ static __global__ void reduce_splits_kernel(int i_begin, int i_end, int ld, int 
   for (int c = 0; c < 6; ++c) dst[c][o] = sum[c];
 }
 
+// One field of reduce_splits_kernel: out[index ? index[i] : i] = sum over
+// the S splits of P[(s*6 + c)*ld + i], for the field c whose [ld] block of
+// split 0 is Pc.  Same summation order as split_sums, so the same bits.
+// Lets a caller copy each finished field to the host while the next one
+// reduces.
+static __global__ void reduce_split_field_kernel(int i_begin, int i_end, int ld, int S,
+                                                 const double* __restrict__ Pc,
+                                                 double* __restrict__ out,
+                                                 const int* __restrict__ index = nullptr) {
+  const int i = i_begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i_end) return;
+  double sum = 0.0;
+#pragma unroll 8
+  for (int s = 0; s < S; ++s) sum += Pc[static_cast<size_t>(s) * 6 * ld + i];
+  out[index ? index[i] : i] = sum;
+}
+
 // Initial step criterion min_i eta0 |a| / |j| (published via ctl).
 static __global__ void initialdt_kernel(int n, int ld, const double* __restrict__ D, StepCtl* ctl,
                                  double eta0) {
