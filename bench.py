@@ -266,7 +266,7 @@ def run_arm(w, precision, state, torch, dist, world, dev, steps, warmup, variant
         "dE_over_E": de,
         "t_end": t_end,
         "E0": T0 + U0,
-        "tiling": {k: tm[k] for k in ("threads", "i_per_thread", "j_tile", "split_j")},
+        "tiling": {k: tm[k] for k in ("threads", "i_per_thread", "j_tile", "split_j", "j_cluster")},
         "tiling_source": {1: "heuristic", 2: "autotuned", 3: "autotuned (cached)"}.get(tm["tiling_source"]),
         "clocks": clk.summary(),
         "launches": int(launches),

@@ -86,6 +86,14 @@ typedef struct {
                          the Hilbert curve every this many steps (tile
                          centres and offsets are rebuilt every step);
                          0 = 16                                             */
+  int j_cluster;      /* pair_variant 4 with an explicit shape: CTAs per
+                         thread-block cluster along j (2, 4 or 8), whose
+                         split partials are summed in the cluster through
+                         distributed shared memory (split_j is rounded up
+                         to a multiple); 0 = no cluster.  Measured at
+                         N = 65536 the smaller corrector read cancels the
+                         slower pair pass, so the autotuner does not time
+                         cluster kernels                                    */
 } nbody_config;
 
 typedef struct nbody_engine nbody_engine;
@@ -129,6 +137,8 @@ typedef struct {
                                        pair pass over this engine's bodies
                                        that took the double-single (near)
                                        form; 0 for other kernels            */
+  int j_cluster;                    /* CTAs per thread-block cluster along
+                                       j of the kernel in use (1: none)     */
 } nbody_timers;
 
 /* Fill *cfg with defaults: eps2 = 1e-7, FP64, device 0, adaptive dt,

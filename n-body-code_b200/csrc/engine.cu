@@ -52,6 +52,9 @@ namespace {
 
 constexpr int kPad = 256;        // body padding granularity (multiple of every j-tile)
 constexpr int kMaxSplit = 64;    // split-j upper bound
+// Rate at which the corrector sums split partials (64 splits at N = 65536:
+// 201 MB in 52 us), the autotuner's price for each partial a tiling leaves.
+constexpr double kSplitSumBytesPerMs = 3.9e9;
 constexpr int kBlockO1 = 256;    // threads per CTA of the O(N) kernels
 constexpr int kMaxBBoxParts = 512;  // CTAs of the bounding-box pass
 constexpr int kOrderBits = 48;     // Hilbert key width (order_key_kernel)
@@ -98,6 +101,7 @@ struct PairKernel {
   size_t smem;  // dynamic shared memory: two j-tile buffers (+ FP64 accumulators)
   int acc_smem = 0, junroll = 2, minb = 1;
   int near = 0;  // tile-relative: 1 = near tiles in double-single (variant 4), 0 = all far (5)
+  int cluster = 1;  // CTAs per thread-block cluster along j (splits summed in the cluster)
 };
 
 template <int NT, int IPT, int TJ, int JU = 2, int MINB = 1>
@@ -126,8 +130,17 @@ PairKernel make_mixed_nf() {
           MINB, NEAR ? 1 : 0};
 }
 
-// The first entry of each shape/variant is the one explicit tilings select;
-// the autotuner times all of them.
+// Near/far rows on clusters of CL CTAs along j: split count a multiple of CL,
+// S / CL partials (pair_mixed_nf_cluster_kernel).
+template <int NT, int IPT, int TJ, int JU, int MINB, int NEAR, int CL>
+PairKernel make_mixed_nf_cl() {
+  return {NBODY_MIXED, NT, IPT, TJ, kRecRel,
+          reinterpret_cast<const void*>(&pair_mixed_nf_cluster_kernel<NT, IPT, TJ, JU, MINB, NEAR, CL>),
+          2 * (TJ + 1) * sizeof(JBodyNF) + sizeof(double) * 6 * IPT * NT, 1, JU, MINB, 1, CL};
+}
+
+// The first entry of each shape/variant is the one explicit tilings select
+// (never a cluster kernel); the autotuner times all of them.
 const std::vector<PairKernel>& registry() {
   static const std::vector<PairKernel> r = {
       make_fp64<128, 2, 128, 1>(),  make_fp64<128, 2, 128, 2>(),  make_fp64<128, 1, 128, 4>(),
@@ -147,6 +160,10 @@ const std::vector<PairKernel>& registry() {
       // the same kernel with every tile taken as far (plain tile-relative
       // separations; pair_variant 5, a measured comparison)
       make_mixed_nf<128, 4, 128, 1, 2, 4, 0>(), make_mixed_nf<128, 2, 128, 1, 1, 1, 0>(),
+      // near/far on thread-block clusters along j (fewer split partials;
+      // selected by nbody_config.j_cluster, not by the autotuner)
+      make_mixed_nf_cl<128, 4, 128, 2, 4, 2, 8>(), make_mixed_nf_cl<128, 4, 128, 2, 4, 2, 4>(),
+      make_mixed_nf_cl<128, 4, 128, 2, 4, 2, 2>(),
       // packed pairs, FP64 accumulators in shared memory (default)
       make_mixed_x2<128, 4, 128, 1, 1>(), make_mixed_x2<256, 4, 128, 1, 1>(),
       make_mixed_x2<128, 4, 128, 1, 2>(), make_mixed_x2<64, 4, 128, 1, 1>(),
@@ -169,12 +186,13 @@ const std::vector<PairKernel>& registry() {
 // hi/lo pairs with shared-memory FP64 accumulators (falling back to
 // register accumulators where that shape has none), 4 = near/far
 // tile-relative, 5 = tile-relative with every tile taken as far.
-const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant) {
+const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int variant,
+                              int cluster = 1) {
   auto match = [&](int fmt, int acc, int near = 1) -> const PairKernel* {
     for (const auto& k : registry())
       if (k.precision == precision && k.nt == nt && k.ipt == ipt && k.tj == tj &&
           (fmt < 0 || k.fmt == fmt) && (acc < 0 || k.acc_smem == acc) &&
-          (k.fmt != kRecRel || k.near == near))
+          (k.fmt != kRecRel || k.near == near) && k.cluster == cluster)
         return &k;
     return nullptr;
   };
@@ -190,9 +208,13 @@ const PairKernel* find_kernel(int precision, int nt, int ipt, int tj, int varian
 
 struct Tiling {
   const PairKernel* k = nullptr;
-  int split = 1;
+  int split = 1;   // CTAs along j
   int source = 0;  // nbody_timers.tiling_source: 1 heuristic/explicit, 2 timed, 3 cached
 };
+
+// Split partials a launch of tiling t leaves in P (cluster kernels sum their
+// CL CTAs' partials into one).
+int partial_count(const Tiling& t) { return t.split / t.k->cluster; }
 
 // Autotune results shared by all engines of the process: (device, precision,
 // record format, ld, rows) -> tiling.
@@ -429,9 +451,13 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
     const PairKernel& k = reg[idx];
     if (k.precision != e->cfg.precision || k.fmt != default_format(e)) continue;
     if (k.fmt == kRecRel && !k.near) continue;  // the automatic choice keeps near tiles exact
+    // cluster kernels save in the split sums what their pair pass loses
+    // (N = 65536: 4.071 vs 4.071 ms with the sums priced in); not timed
+    if (k.cluster > 1) continue;
     const int s0 = choose_split(e, k, rows);
     NB_TRY(launch_pack(e, e->n, own_inputs(e), e->stream, k.fmt, k.tj));
     for (int s : {std::max(1, s0 / 2), s0, std::min(kMaxSplit, s0 * 2)}) {
+      s = std::min(kMaxSplit, (s + k.cluster - 1) / k.cluster * k.cluster);
       NB_TRY(ensure_partials(e, s));
       Tiling t{&k, s};
       NB_TRY(launch_pair(e, t, 0, rows, e->stream));  // warm-up
@@ -439,11 +465,16 @@ nbody_status autotune(nbody_engine* e, int rows, Tiling* out) {
       for (int r = 0; r < 3; ++r) NB_TRY(launch_pair(e, t, 0, rows, e->stream));
       NB_CUDA(cudaEventRecord(b, e->stream));
       NB_CUDA(cudaEventSynchronize(b));
-      float ms = 0.f;
-      NB_CUDA(cudaEventElapsedTime(&ms, a, b));
+      float pair_ms = 0.f;
+      NB_CUDA(cudaEventElapsedTime(&pair_ms, a, b));
+      pair_ms /= 3;
+      // the split partials are summed after every pass (corrector or
+      // reduction): 48 bytes per row and partial at the measured 3.9 TB/s
+      const float ms = pair_ms + static_cast<float>(48.0 * (s / k.cluster) * rows / kSplitSumBytesPerMs);
       if (getenv("NBODY_TUNE_VERBOSE"))
-        fprintf(stderr, "[nbody tune] #%zu prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d minb=%d split=%d  %.4f ms\n",
-                idx, k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, k.minb, s, ms / 3);
+        fprintf(stderr, "[nbody tune] #%zu prec=%d rows=%d nt=%d ipt=%d tj=%d fmt=%d acc_smem=%d ju=%d minb=%d cluster=%d split=%d  %.4f ms (pair %.4f)\n",
+                idx, k.precision, rows, k.nt, k.ipt, k.tj, k.fmt, k.acc_smem, k.junroll, k.minb,
+                k.cluster, s, ms, pair_ms);
       if (ms < best) {
         best = ms;
         best_idx = static_cast<int>(idx);
@@ -477,16 +508,19 @@ nbody_status get_tiling(nbody_engine* e, int rows, Tiling* out) {
                            : rel ? (rows < 8192 ? 2 : 4)
                                  : (c.precision == NBODY_FP64 && rows < 32768 ? 1 : 2);
   int tj = c.j_tile ? c.j_tile : 128;
-  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, variant);
+  const int cl = c.j_cluster > 1 ? c.j_cluster : 1;
+  const PairKernel* k = find_kernel(c.precision, nt, ipt, tj, variant, cl);
   if (!k)
     return fail(NBODY_ERR_INVALID_ARG,
                 "no compiled pair kernel for threads=%d i_per_thread=%d j_tile=%d variant=%d", nt,
                 ipt, tj, variant);
-  const bool automatic = !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j && !c.pair_variant;
+  const bool automatic = !c.threads && !c.i_per_thread && !c.j_tile && !c.split_j &&
+                         !c.pair_variant && !c.j_cluster;
   if (c.tune && automatic) return autotune(e, rows, out);
   if (e->tune_lookup && automatic && tuned_lookup(e, rows, out)) return NBODY_OK;
   out->k = k;
   out->split = c.split_j ? std::min(c.split_j, kMaxSplit) : choose_split(e, *k, rows);
+  out->split = std::min(kMaxSplit, (out->split + cl - 1) / cl * cl);  // whole clusters
   out->source = 1;
   return NBODY_OK;
 }
@@ -615,7 +649,7 @@ nbody_status eval_foreign_rel(nbody_engine* e, const Tiling& t, int n, const SoA
   NB_TRY(launch_pair(e, t, 0, n, st, &sorted, n));
   if (!reduce) return NBODY_OK;  // the caller sums the splits (rows in sort_idx + ld order)
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      0, n, e->ld, t.split, e->P, out, nullptr, ord);
+      0, n, e->ld, partial_count(t), e->P, out, nullptr, ord);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
@@ -658,7 +692,7 @@ nbody_status eval_current(nbody_engine* e) {
   NB_CUDA(cudaEventRecord(e->ev_init[0], e->stream));
   NB_TRY(launch_pair(e, e->tiling, 0, e->n, e->stream));
   reduce_splits_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
-      0, e->n, e->ld, e->tiling.split, e->P, own_derivs(e));
+      0, e->n, e->ld, partial_count(e->tiling), e->P, own_derivs(e));
   NB_CUDA(cudaGetLastError());
   NB_CUDA(cudaEventRecord(e->ev_init[1], e->stream));
   if (e->cfg.dt <= 0.0) {
@@ -683,7 +717,7 @@ nbody_status enqueue_predict(nbody_engine* e, cudaStream_t st) {
 
 nbody_status enqueue_correct(nbody_engine* e, cudaStream_t st) {
   correct_kernel<<<(e->n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      e->n, e->ld, e->tiling.split, e->P, e->X, e->V, e->D, e->ctl, e->cfg.eta);
+      e->n, e->ld, partial_count(e->tiling), e->P, e->X, e->V, e->D, e->ctl, e->cfg.eta);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
@@ -830,6 +864,9 @@ nbody_status nbody_create(nbody_engine** out, const nbody_config* cfg) {
     return fail(NBODY_ERR_INVALID_ARG, "negative tiling parameter");
   if (cfg->pair_variant < 0 || cfg->pair_variant > 5)
     return fail(NBODY_ERR_INVALID_ARG, "pair_variant = %d", cfg->pair_variant);
+  if (cfg->j_cluster != 0 && cfg->j_cluster != 1 && cfg->j_cluster != 2 && cfg->j_cluster != 4 &&
+      cfg->j_cluster != 8)
+    return fail(NBODY_ERR_INVALID_ARG, "j_cluster = %d (0, 1, 2, 4 or 8)", cfg->j_cluster);
   if (cfg->sort_every < 0) return fail(NBODY_ERR_INVALID_ARG, "sort_every = %d", cfg->sort_every);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1092,6 +1129,7 @@ nbody_status nbody_get_timers(nbody_engine* e, nbody_timers* out) {
     out->i_per_thread = e->tiling.k->ipt;
     out->j_tile = e->tiling.k->tj;
     out->split_j = e->tiling.split;
+    out->j_cluster = e->tiling.k->cluster;
     out->record_format = e->tiling.k->fmt;
     out->tiling_source = e->tiling.source;
     const PairKernel& k = *e->tiling.k;
@@ -1160,7 +1198,7 @@ nbody_status nbody_acc_jerk_device(nbody_engine* e, int n, const double* x, cons
   NB_TRY(launch_pack(e, n, in, st, t.k->fmt, t.k->tj));
   NB_TRY(launch_pair(e, t, 0, n, st, &in, n));
   reduce_splits_kernel<<<(n + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, st>>>(
-      0, n, e->ld, t.split, e->P, out);
+      0, n, e->ld, partial_count(t), e->P, out);
   NB_CUDA(cudaGetLastError());
   return NBODY_OK;
 }
@@ -1308,7 +1346,7 @@ extern "C" nbody_status nbody_force_calculation(int n, double eps2, int precisio
     if (i_end < n) memset(out[k] + i_end, 0, sizeof(double) * (n - i_end));
     if (!rows) continue;
     reduce_split_field_kernel<<<(rows + kBlockO1 - 1) / kBlockO1, kBlockO1, 0, e->stream>>>(
-        i_begin, i_end, e->ld, t.split, e->P + k * ld, e->D + k * ld, index);
+        i_begin, i_end, e->ld, partial_count(t), e->P + k * ld, e->D + k * ld, index);
     NB_CUDA(cudaGetLastError());
     NB_CUDA(cudaEventRecord(e->aux_ev[0], e->stream));
     NB_CUDA(cudaStreamWaitEvent(e->aux, e->aux_ev[0], 0));

@@ -35,6 +35,7 @@
 //          warp's rows and is formed in double-single for near tiles
 //          (RowsMixedNF below), so close pairs keep the hi/lo accuracy.
 #pragma once
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "tma.cuh"
@@ -819,6 +820,53 @@ __global__ void __launch_bounds__(NT, MINB) pair_mixed_nf_kernel(const JBodyNF* 
   r.store(a.out + static_cast<size_t>(blockIdx.y) * 6 * a.stride, a.stride, a.i_end);
   // near tiles of this launch, counted per warp (the unit that classifies)
   if (NEAR && a.near_count && (threadIdx.x & 31) == 0 && r.near_tiles)
+    atomicAdd(a.near_count, static_cast<unsigned long long>(r.near_tiles));
+}
+
+// The near/far kernel on thread-block clusters of CL CTAs along the j-split
+// dimension: the CTAs of a cluster share a row block and take consecutive
+// j-ranges, then sum their FP64 accumulators (shared memory) through
+// distributed shared memory, in rank order, and write one split partial per
+// cluster (split index blockIdx.y / CL).  The corrector then reads S / CL
+// partials instead of S.  Each CTA sums a 1/CL slice of the entries.  Every
+// CTA reaches both cluster barriers: a timed-out tile wait sets the status
+// word and ends only the tile loop, so no CTA leaves the others waiting.
+template <int NT, int IPT, int TJ, int JU, int MINB, int NEAR, int CL>
+__global__ void __cluster_dims__(1, CL, 1) __launch_bounds__(NT, MINB)
+    pair_mixed_nf_cluster_kernel(const JBodyNF* __restrict__ jt, PairArgs a) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t full[2];
+  using R = RowsMixedNF<NT, IPT, TJ, 1, JU, NEAR>;
+  constexpr int kRecs = TJ + 1;
+  TilePipe<JBodyNF, kRecs> pipe;
+  pipe.init(reinterpret_cast<JBodyNF*>(smem_raw), full);
+  const int row0 = a.i_begin + blockIdx.x * R::ROWS;
+  const int t_begin = blockIdx.y * a.tiles_per_split;
+  const int nt = max(0, min(a.tiles_per_split, a.n_tiles - t_begin));
+  R r;
+  r.begin_rows(a.rows, row0, a.n_rows_pad - 1, a.i_end, a.eps2,
+               smem_raw + 2 * kRecs * sizeof(JBodyNF));
+  const bool ok = pipe.run(jt + static_cast<size_t>(t_begin) * kRecs, nt, a.status,
+                           [&](const JBodyNF* tile) { r.consume(tile); });
+  cg::cluster_group cluster = cg::this_cluster();
+  cluster.sync();  // every CTA's accumulators are final and visible to the cluster
+  const unsigned q = cluster.block_rank();
+  const double* acc[CL];
+#pragma unroll
+  for (int p = 0; p < CL; ++p) acc[p] = cluster.map_shared_rank(r.acc_sm, p);
+  double* out = a.out + static_cast<size_t>(blockIdx.y / CL) * 6 * a.stride;
+  constexpr int kEntries = 6 * IPT * NT;  // acc_sm[(c * IPT + k) * NT + thread]
+  for (int e = static_cast<int>(q) * NT + threadIdx.x; e < kEntries; e += CL * NT) {
+    double s = 0.0;
+#pragma unroll
+    for (int p = 0; p < CL; ++p) s += acc[p][e];
+    const int c = e / (IPT * NT), k = (e / NT) % IPT, t = e % NT;
+    const int i = row0 + (t >> 5) * 32 * IPT + 32 * k + (t & 31);  // RowsMixedNF::row_of
+    if (i < a.i_end) out[static_cast<size_t>(c) * a.stride + i] = s;
+  }
+  cluster.sync();  // peers keep their shared memory until every slice is read
+  if (NEAR && ok && a.near_count && (threadIdx.x & 31) == 0 && r.near_tiles)
     atomicAdd(a.near_count, static_cast<unsigned long long>(r.near_tiles));
 }
 

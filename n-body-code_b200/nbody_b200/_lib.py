@@ -47,6 +47,7 @@ class NBodyConfig(C.Structure):
         ("split_j", C.c_int),
         ("pair_variant", C.c_int),
         ("sort_every", C.c_int),
+        ("j_cluster", C.c_int),
     ]
 
 
@@ -71,6 +72,7 @@ class NBodyTimers(C.Structure):
         ("dt_crit", C.c_double),
         ("tiling_source", C.c_int),
         ("near_tile_fraction", C.c_double),
+        ("j_cluster", C.c_int),
     ]
 
 

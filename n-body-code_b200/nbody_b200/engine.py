@@ -45,7 +45,8 @@ class Engine:
     def __init__(self, n: int, eps2: float = 1e-7, precision: str = "fp64", device: int = 0,
                  dt: float | None = None, eta: float = 1e-2, eta0: float = 1e-4,
                  tune: bool = False, threads: int = 0, i_per_thread: int = 0, j_tile: int = 0,
-                 split_j: int = 0, pair_variant: int = 0, sort_every: int = 0):
+                 split_j: int = 0, pair_variant: int = 0, sort_every: int = 0,
+                 j_cluster: int = 0):
         L = _lib.load()
         cfg = NBodyConfig()
         check(L.nbody_config_init(C.byref(cfg)), "nbody_config_init")
@@ -60,6 +61,7 @@ class Engine:
         cfg.threads, cfg.i_per_thread, cfg.j_tile, cfg.split_j = threads, i_per_thread, j_tile, split_j
         cfg.pair_variant = pair_variant
         cfg.sort_every = sort_every
+        cfg.j_cluster = j_cluster
         h = C.c_void_p()
         check(L.nbody_create(C.byref(h), C.byref(cfg)), "nbody_create")
         self._h = h

@@ -488,6 +488,38 @@ def test_tile_relative_small_and_ragged(n):
     assert ea.max() <= 2e-4, ea.max()
 
 
+@pytest.mark.parametrize("cl", [2, 4, 8])
+def test_near_far_on_thread_block_clusters(cl):
+    """pair_variant 4 on clusters of cl CTAs along j (j_cluster): the CTAs of
+    a cluster sum their split partials through distributed shared memory
+    before one partial per cluster is written.  Same terms as the one-CTA
+    kernel with the split sums associated differently, so the two agree to
+    FP64 rounding; a split count that is not a multiple of cl is rounded up;
+    Hermite steps (graph-captured) follow the one-CTA engine."""
+    n, eps2 = 20000, 1e-4
+    s = nb.plummer(n, seed=12)
+    shape = dict(pair_variant=4, threads=128, i_per_thread=4, j_tile=128)
+    base = engine_derivs(s, eps2, precision="mixed", split_j=16, **shape)
+    for split in (16, 10):
+        d = engine_derivs(s, eps2, precision="mixed", split_j=split, j_cluster=cl, **shape)
+        ea, ej = derivs_rel(d, base)
+        assert ea <= 1e-10 and ej <= 1e-10, (cl, split, ea, ej)
+    rows = np.arange(0, n, 97)
+    ea, _ = derivs_rel(d[:, rows], O.force_rows(s, eps2, rows))
+    assert ea <= 2e-6, ea
+    runs = {}
+    for name, kw in (("one", {}), ("cluster", dict(j_cluster=cl))):
+        with nb.Engine(n, eps2=eps2, precision="mixed", dt=1.0 / 1024, split_j=16, **shape, **kw) as e:
+            e.set_state(s)
+            e.force_calculation()
+            e.timestepping(8)
+            runs[name] = e.get_state()
+            tm = e.timers()
+    assert tm["split_j"] == 16
+    dx = max(np.abs(runs["cluster"][k] - runs["one"][k]).max() for k in ("x", "y", "z"))
+    assert dx <= 1e-12, dx
+
+
 def test_tile_relative_deterministic_and_order_free():
     """Bitwise reproducible (stable sort, fixed reduction order); the result
     does not depend on the order the bodies are given in."""
@@ -567,7 +599,7 @@ def test_autotuned_engine_parity_and_reuse(n, precision):
             e.force_calculation()
             runs.append((e.get_derivs(), e.timers()))
     (d, t1), (d2, t2) = runs
-    keys = ("threads", "i_per_thread", "j_tile", "split_j", "record_format")
+    keys = ("threads", "i_per_thread", "j_tile", "split_j", "j_cluster", "record_format")
     print(f"n={n} {precision}: tuned tiling {[t1[k] for k in keys]} (source {t1['tiling_source']})")
     assert t1["tiling_source"] in (2, 3)      # timed here, or by an earlier engine of this size
     assert t2["tiling_source"] == 3           # the second engine reuses the cached choice
