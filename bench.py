@@ -817,7 +817,8 @@ def large_n_block(a, peaks, torch, dev):
     for k, arm in arms.items():
         prec = "fp64" if k == "fp64" else "mixed"
         out[k] = {"value": inter / (arm["ms_per_step"] * 1e-3) / 1e9, "unit": "Gint/s",
-                  "ms_per_step": arm["ms_per_step"], "pair_ms": arm["pair_ms"],
+                  "ms_per_step": arm["ms_per_step"], "steps_per_s": 1e3 / arm["ms_per_step"],
+                  "pair_ms": arm["pair_ms"],
                   "kernel": KERNEL_NAMES[arm["record_format"]], "tiling": arm["tiling"],
                   "tiling_source": arm["tiling_source"], "roofline": roofline(peaks, w, arm, prec),
                   "clocks": arm["clocks"]}
@@ -906,7 +907,8 @@ def main():
         variant_used = 5
     line = {
         "metric": METRIC, "value": value, "unit": "Gint/s", "n_gpus": world, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": a.warmup, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "higher_is_better": True,
+        "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64",
         "data": "synthetic (seeded Plummer sphere, Henon units)",
         "config": {"workload": w.name(a.precision), "n": w.n, "eps": w.eps, "dt": w.dt,
@@ -927,7 +929,8 @@ def main():
     }
     if other is not None:
         ov = replica_value(world, inter, other["ms_per_step"])
-        line[other_prec] = {"value": ov, "ms_per_step": other["ms_per_step"], "pair_ms": other["pair_ms"],
+        line[other_prec] = {"value": ov, "ms_per_step": other["ms_per_step"],
+                            "steps_per_s": 1e3 / other["ms_per_step"], "pair_ms": other["pair_ms"],
                             "roofline": roofline(peaks, w, other, other_prec), "tiling": other["tiling"],
                             "tiling_source": other["tiling_source"], "clocks": other["clocks"]}
         line["energy_error"][other_prec] = other["dE_over_E"]
